@@ -1,0 +1,318 @@
+"""Benchmark of the Fire-X simulation step on B200 (one JSON line on stdout, rank 0).
+
+Workload (the HD tier the headline metric is quoted on): grid 128x192x128 (3,145,728
+cells), plain FP32, sphere emitter r=14 cells at (64,12,64) injecting fuel 1.0 and
+1500 K with a seeded +-10 % per-step jitter, velocity noise +-0.05, dt = 1/60 s,
+96 primary + 96 residual Jacobi sweeps per step. Inputs are synthetic (no dataset).
+
+A bench "step" is one full simulation step. ``value`` = cells x steps x ranks / device
+seconds (max over ranks) with all state resident in HBM; ``e2e`` is the same metric
+through the C ABI with, every step, the per-step parameter block going host -> device and
+the resulting flow field (16 B/cell) read back into pinned host memory. The roofline
+object is for the dominant kernel (the Jacobi sweep), timed with CUDA events on the
+simulation's own stream inside the timed region.
+
+``--impl reference`` times the CPU restatement of the reference step (oracle/, OpenMP on
+all host cores) on the same workload: the reference itself is WGSL for WebGPU and cannot
+run on this machine (no WebGPU implementation, no graphics stack, no JS runtime).
+
+Multi-GPU (torchrun): each rank steps its own independent replica (weak scaling; the
+step has no cross-rank exchange); barrier + synchronize around the timed region and the
+max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+DIMS = (128, 192, 128)
+P_ITERS = R_ITERS = 96
+DT = 1.0 / 60.0
+SPHERE = dict(center=(64.0, 12.0, 64.0), radius=14.0, fuel=1.0, temperature=1500.0)
+SEED = 20251203
+METRIC = "Gcell-steps/s"
+WORKLOAD = "fire-x step, HD tier 128x192x128, plain FP32, sphere r=14 @ (64,12,64), +-10% jitter, 96+96 Jacobi, dt=1/60"
+JACOBI_BYTES_PER_CELL = 12  # read p + read div + write p, f32 (algorithmic, per sweep)
+L2_BYTES = 126 * 1024 * 1024
+
+
+def cells() -> int:
+    return DIMS[0] * DIMS[1] * DIMS[2]
+
+
+def options(make_options):
+    return make_options(pressure_iterations=P_ITERS, correction_iterations=R_ITERS, seed=SEED, velocity_noise=0.05,
+                        emission_jitter=0.1, spheres=[SPHERE])
+
+
+def config(extra=None) -> dict:
+    c = {"workload": WORKLOAD, "grid": list(DIMS), "cells": cells(), "jacobi": [P_ITERS, R_ITERS], "dt": DT,
+         "l2": "inputs larger than L2: 365 MB of resident step state per replica vs 126 MB L2",
+         "parallelism": "replicas (one independent simulation per GPU)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                parts = [p.strip() for p in out.stdout.strip().split(",")]
+                if len(parts) >= 9:
+                    self.samples.append(parts)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_baseline_sample(budget_s: float = 20.0) -> dict:
+    """The CPU oracle (restatement of the reference step) on this host's cores: one warm-up
+    step, then as many full HD steps as fit in about budget_s seconds (at least one)."""
+    from fire_b200.sim import make_options
+    from oracle import oracle as O
+    O.build()
+    sim = O.OracleSim(DIMS, options(make_options))
+    sim.step(1, DT)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        sim.step(1, DT)
+        n += 1
+        el = time.perf_counter() - t0
+        if el + el / n > budget_s:
+            break
+    sim.close()
+    return {"value": cells() * n / el / 1e9, "unit": METRIC, "cores": O.num_threads(), "kind": "port",
+            "sample": f"{n} full HD steps (96+96) after 1 warm-up, {el:.1f} s, OpenMP over z-slabs",
+            "ms_per_step": el / n * 1e3}
+
+
+def run_reference(args) -> None:
+    """--impl reference: the CPU restatement of the reference path on this host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from fire_b200.sim import make_options
+    from oracle import oracle as O
+    O.build()
+    sim = O.OracleSim(DIMS, options(make_options))
+    for _ in range(min(args.warmup, 1)):
+        sim.step(1, DT)
+    budget = float(os.environ.get("FIREX_REFERENCE_BUDGET_S", "90"))
+    times = []
+    t_start = time.perf_counter()
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        sim.step(1, DT)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start + times[-1] > budget:
+            break
+    el = sum(times)
+    n = len(times)
+    value = cells() * n / el / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": el / n * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config({"reference_path": "CPU restatement of src/sim/firex WGSL step (oracle/firex_oracle.cpp)"}),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": O.num_threads(), "kind": "port",
+                         "sample": f"{n} of {args.steps} requested HD steps (budget {budget:.0f} s)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "p50_step_ms": statistics.median(times) * 1e3,
+        "p99_step_ms": sorted(times)[min(n - 1, int(math.ceil(0.99 * n)) - 1)] * 1e3,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def percentile(xs, q):
+    s = sorted(xs)
+    return s[min(len(s) - 1, max(0, int(math.ceil(q * len(s))) - 1))]
+
+
+def run_gpu(args) -> None:
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from fire_b200.sim import FireXSim, make_options
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sim = FireXSim(DIMS, options(make_options))
+    stream = torch.cuda.ExternalStream(sim.stream)
+    n_cells = cells()
+
+    # ---- warm-up ----
+    sim.step(args.warmup, DT)
+    sim.sync()
+
+    # ---- device-resident timed region ----
+    sim.set_profiling(True)
+    sim.pass_times()  # clear
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev) as clk:
+        evs[0].record(stream)
+        for i in range(args.steps):
+            sim.step(1, DT)
+            evs[i + 1].record(stream)
+        sim.sync()
+        torch.cuda.synchronize()
+    barrier()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    passes = sim.pass_times()
+    sim.set_profiling(False)
+    total_ms_max = max_over_ranks(total_ms)
+    value = n_cells * args.steps * world / (total_ms_max / 1e3) / 1e9
+
+    # ---- end-to-end through the C ABI with host buffers ----
+    pinned = torch.empty((DIMS[2], DIMS[1], DIMS[0], 4), dtype=torch.float32, pin_memory=True)
+    host = pinned.numpy()
+    e2e_steps = max(1, min(args.steps, 30))
+    sim.step(1, DT)
+    sim.read_into("flow", host)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        sim.step(1, DT)
+        sim.read_into("flow", host)
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = n_cells * e2e_steps * world / t_e2e / 1e9
+    assert np.isfinite(host).all()
+
+    # ---- roofline of the dominant kernel ----
+    jac_ms, jac_n = passes["jacobi"]
+    jac_avg_ms = jac_ms / max(1, jac_n)
+    peak, peak_kind = measured_peak_hbm()
+    achieved = JACOBI_BYTES_PER_CELL * n_cells / (jac_avg_ms / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "jacobi_f32_traffic.json"
+    if tp.exists():
+        try:
+            traffic = json.loads(tp.read_text()).get("bytes_per_launch_hd")
+        except Exception:
+            traffic = None
+    launches = sum(n for _, n in passes.values())
+
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline_sample(float(os.environ.get("FIREX_CPU_BASELINE_S", "20")))
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(),
+            "p50_step_ms": percentile(step_ms, 0.5), "p99_step_ms": percentile(step_ms, 0.99),
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 384,
+                    "d2h_bytes_per_step": n_cells * 16, "steps": e2e_steps,
+                    "what": "firex_step (384 B parameter block host->device) + firex_read_field(FLOW) into pinned host memory, every step"},
+            "roofline": {"kernel": "fxk_jacobi_f32", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                         "traffic": traffic, "bytes_per_cell": JACOBI_BYTES_PER_CELL, "avg_launch_us": jac_avg_ms * 1e3,
+                         "launches": jac_n},
+            "passes_ms_per_step": {k: v[0] / args.steps for k, v in passes.items()},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fire_b200", choices=["fire_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl != "reference":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,104 @@
+// fx_device.cuh — device-side building blocks shared by the Fire-X kernels.
+//
+// The WGSL builtins are written from their WGSL-spec definitions so the f32 kernels
+// evaluate every reference expression as the same sequence of IEEE operations:
+//   max(a,b) = (a < b) ? b : a          min(a,b) = (b < a) ? b : a
+//   clamp(x,lo,hi) = min(max(x,lo),hi)  mix(a,b,t) = a*(1-t) + b*t
+//   smoothstep(e0,e1,x) = t*t*(3-2t), t = clamp((x-e0)/(e1-e0), 0, 1)
+// Files that include this header for the reference-faithful path are compiled with
+// --fmad=false (no contraction into fused multiply-add).
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+
+#include "../../include/firex.h"
+
+// Per-step parameter block: the reference's 44-float uniform block (shaders.ts:2-14,
+// written by FireXEngine.writeUniforms, FireXEngine.ts:2043-2113) followed by the
+// sphere-emitter extension.
+struct FxParams {
+    float u[FIREX_UNIFORM_FLOATS];
+    int32_t emitter_mode;
+    float jitter;
+    int32_t num_spheres;
+    int32_t pad;
+    firex_sphere spheres[FIREX_MAX_SPHERES];
+};
+
+// Uniform slots (vec4 members of Parameters, shaders.ts:2-14).
+enum FxSlot {
+    U_GRID_X = 0, U_GRID_Y = 1, U_GRID_Z = 2,
+    U_DT = 4, U_TIME = 5,
+    U_FUEL_RATE = 8, U_OXYGEN = 9, U_HEAT_EFF = 10, U_VORTICITY = 11,
+    U_T_AMBIENT = 15,
+    U_AIM_HEIGHT = 25,
+    U_BURNER_X = 28, U_BURNER_Z = 29, U_THICKNESS = 30, U_FIRE_POWER = 31,
+    U_DOMAIN_X = 32, U_DOMAIN_Y = 33, U_DOMAIN_Z = 34,
+    U_LIFT = 36, U_BUOYANCY = 37, U_PERSISTENCE = 38,
+    U_ENTRAIN = 40, U_CINEMATIC = 42,
+};
+
+#define FXD __device__ __forceinline__
+
+FXD float fx_max(float a, float b) { return (a < b) ? b : a; }
+FXD float fx_min(float a, float b) { return (b < a) ? b : a; }
+FXD float fx_clamp(float x, float lo, float hi) { return fx_min(fx_max(x, lo), hi); }
+FXD float fx_mix(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+FXD float fx_smoothstep(float e0, float e1, float x) {
+    float t = fx_clamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+FXD float4 fx_mix4(float4 a, float4 b, float t) {
+    return make_float4(fx_mix(a.x, b.x, t), fx_mix(a.y, b.y, t), fx_mix(a.z, b.z, t), fx_mix(a.w, b.w, t));
+}
+FXD float fx_length3(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
+
+// Float constant rounded from its double literal, as WGSL concretises abstract floats.
+#define FC(v) (static_cast<float>(v))
+
+struct FxGrid {
+    int X, Y, Z;
+    __device__ __forceinline__ long long idx(int x, int y, int z) const {
+        x = x < 0 ? 0 : (x > X - 1 ? X - 1 : x);
+        y = y < 0 ? 0 : (y > Y - 1 ? Y - 1 : y);
+        z = z < 0 ? 0 : (z > Z - 1 ? Z - 1 : z);
+        return (long long)x + (long long)X * ((long long)y + (long long)Y * (long long)z);
+    }
+};
+
+// domainExtent() and cellMetric() (shaders.ts:35-41).
+FXD float3 fx_extent(const float* u) {
+    return make_float3(fx_max(u[U_DOMAIN_X], 0.001f), fx_max(u[U_DOMAIN_Y], 0.001f), fx_max(u[U_DOMAIN_Z], 0.001f));
+}
+FXD float3 fx_metric(const float* u) {
+    float3 e = fx_extent(u);
+    return make_float3(u[U_GRID_X] / e.x, u[U_GRID_Y] / e.y, u[U_GRID_Z] / e.z);
+}
+
+// Sphere emitter mask (extension): |c + 0.5 - center|^2 <= r^2, float, fixed order.
+// Written with explicit round-to-nearest intrinsics so the integer mask is the same in
+// every translation unit, whatever its contraction flags.
+FXD bool fx_sphere_inside(const firex_sphere& s, int x, int y, int z) {
+    float dx = __fsub_rn(__fadd_rn((float)x, 0.5f), s.center[0]);
+    float dy = __fsub_rn(__fadd_rn((float)y, 0.5f), s.center[1]);
+    float dz = __fsub_rn(__fadd_rn((float)z, 0.5f), s.center[2]);
+    float d2 = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    return d2 <= __fmul_rn(s.radius, s.radius);
+}
+
+// splitmix64 (Steele, Lea, Flood 2014) for the seeded initial velocity noise.
+FXD uint64_t fx_splitmix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Seeded initial velocity noise (extension): component comp of cell id, uniform in
+// [-a, a] from 24 random bits.
+FXD float fx_velocity_noise(uint64_t seed, uint64_t cell, int comp, float a) {
+    uint64_t h = fx_splitmix64(fx_splitmix64(seed ^ 0x6A09E667F3BCC909ull) + cell * 4u + (uint64_t)comp);
+    float u = __fmul_rn((float)(h >> 40), 1.0f / 16777216.0f);
+    return __fmul_rn(a, __fsub_rn(__fmul_rn(2.0f, u), 1.0f));
+}

@@ -1,0 +1,255 @@
+"""Python handle over the C ABI (include/firex.h) of the CUDA library.
+
+``FireXSim`` owns one ``firex_sim*``: create, named parameters, reset, step, field
+readback/upload, divergence norm and counters. Fields come back as numpy arrays in the
+reference layout, shaped (Z, Y, X, 4) for vec4 fields and (Z, Y, X) for scalars
+(cell index x + X*(y + Y*z), shaders.ts:47-51).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+from typing import Iterable, Mapping, Sequence
+
+import numpy as np
+
+from . import _abi as A
+
+_LIB: C.CDLL | None = None
+LIB_PATH = Path(__file__).resolve().parent / "libfirex_b200.so"
+
+
+class FireXError(RuntimeError):
+    """A firex_* call returned a negative status; ``code`` holds it."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Loads the CUDA library (once). Raises if it is missing: there is no fallback."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(
+            f"{p} is missing: build it with `python -m fire_b200.build` (no CPU fallback exists)")
+    lib = C.CDLL(str(p))
+    A.declare_firex(lib)
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def make_options(
+    *,
+    precision: int = A.PRECISION_F32,
+    pressure_mode: int = A.PRESSURE_AUTO,
+    pressure_iterations: int = 64,
+    correction_iterations: int = 64,
+    spheres: Sequence[Mapping[str, object]] | None = None,
+    seed: int = 0,
+    velocity_noise: float = 0.0,
+    emission_jitter: float = 0.0,
+    cinematic: bool = True,
+    jacobi_block: int = 0,
+    memory_budget_bytes: int = 0,
+) -> A.Options:
+    """Options with the library defaults (firex_default_options) plus overrides.
+
+    ``spheres`` switches the emitter to the sphere list; each entry has ``center``
+    (x, y, z in cells), ``radius`` (cells), ``fuel`` and ``temperature`` (K).
+    """
+    o = A.Options()
+    o.precision = precision
+    o.pressure_mode = pressure_mode
+    o.pressure_iterations = pressure_iterations
+    o.correction_iterations = correction_iterations
+    o.emitter_mode = A.EMITTER_BURNER
+    if spheres is not None:
+        if len(spheres) > A.MAX_SPHERES:
+            raise ValueError(f"at most {A.MAX_SPHERES} spheres")
+        o.emitter_mode = A.EMITTER_SPHERES
+        o.num_spheres = len(spheres)
+        for i, s in enumerate(spheres):
+            c = s["center"]
+            o.spheres[i].center[0], o.spheres[i].center[1], o.spheres[i].center[2] = (float(c[0]), float(c[1]), float(c[2]))
+            o.spheres[i].radius = float(s["radius"])
+            o.spheres[i].fuel = float(s.get("fuel", 1.0))
+            o.spheres[i].temperature = float(s.get("temperature", 1500.0))
+    o.seed = seed & 0xFFFFFFFFFFFFFFFF
+    o.velocity_noise = velocity_noise
+    o.emission_jitter = emission_jitter
+    o.cinematic = 1 if cinematic else 0
+    o.jacobi_block = jacobi_block
+    o.memory_budget_bytes = memory_budget_bytes
+    return o
+
+
+class _Handle:
+    """Shared method bodies for any library exporting the firex_* signatures under
+    ``prefix``; the CUDA library uses prefix 'firex_'."""
+
+    prefix = "firex_"
+
+    def __init__(self, lib: C.CDLL, dims: Iterable[int], options: A.Options | None = None, **kw):
+        self._lib = lib
+        self._h = C.c_void_p()
+        self.dims = tuple(int(d) for d in dims)
+        if len(self.dims) != 3:
+            raise ValueError("dims must be (X, Y, Z)")
+        opts = options if options is not None else make_options(**kw)
+        rc = self._fn("create")(A.DIMS(*self.dims), C.byref(opts), C.byref(self._h))
+        if rc != A.OK:
+            msg = self._fn("last_error")(None)
+            raise FireXError(rc, msg.decode() if msg else "create failed")
+        self.options = opts
+        self.cells = self.dims[0] * self.dims[1] * self.dims[2]
+
+    def _fn(self, name: str):
+        return getattr(self._lib, self.prefix + name)
+
+    def _check(self, rc: int) -> None:
+        if rc != A.OK:
+            msg = self._fn("last_error")(self._h)
+            raise FireXError(rc, msg.decode() if msg else "error")
+
+    # -- lifecycle -----------------------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            self._fn("destroy")(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- engine ----------------------------------------------------------------------------
+    def set_parameter(self, name: str, value) -> None:
+        kind = A.VALUE_BOOLEAN if isinstance(value, bool) else A.VALUE_NUMBER
+        self._check(self._fn("set_parameter")(self._h, name.encode(), kind, float(value)))
+
+    def get_parameter(self, name: str) -> float:
+        v = C.c_double()
+        self._check(self._fn("get_parameter")(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def reset(self) -> None:
+        self._check(self._fn("reset")(self._h))
+
+    def step(self, n: int = 1, dt: float = 1.0 / 60.0) -> None:
+        self._check(self._fn("step")(self._h, int(n), float(dt)))
+
+    def sync(self) -> None:
+        self._check(self._fn("sync")(self._h))
+
+    # -- fields ------------------------------------------------------------------------------
+    def _shape(self, field: int):
+        dtype, comps = A.FIELD_LAYOUT[field]
+        X, Y, Z = self.dims
+        shape = (Z, Y, X, comps) if comps > 1 else (Z, Y, X)
+        return np.dtype(dtype), shape
+
+    def read(self, field) -> np.ndarray:
+        f = A.FIELD_NAMES[field] if isinstance(field, str) else int(field)
+        dtype, shape = self._shape(f)
+        out = np.empty(shape, dtype=dtype)
+        self._check(self._fn("read_field")(self._h, f, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def read_into(self, field, out: np.ndarray) -> np.ndarray:
+        f = A.FIELD_NAMES[field] if isinstance(field, str) else int(field)
+        self._check(self._fn("read_field")(self._h, f, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def write(self, field, data: np.ndarray) -> None:
+        f = A.FIELD_NAMES[field] if isinstance(field, str) else int(field)
+        dtype, shape = self._shape(f)
+        arr = np.ascontiguousarray(data, dtype=dtype).reshape(shape)
+        self._check(self._fn("write_field")(self._h, f, arr.ctypes.data_as(C.c_void_p), arr.nbytes))
+
+    def divergence_norm(self) -> tuple[float, float, int]:
+        out = (C.c_double * 3)()
+        self._check(self._fn("divergence_norm")(self._h, out))
+        return out[0], out[1], int(out[2])
+
+    # -- counters ---------------------------------------------------------------------------
+    @property
+    def state(self) -> dict:
+        st = A.State()
+        self._check(self._fn("get_state")(self._h, C.byref(st)))
+        return {
+            "simulation_time": st.simulation_time,
+            "frame_index": st.frame_index,
+            "species_index": st.species_index,
+            "pressure_index": st.pressure_index,
+        }
+
+    def set_state(self, simulation_time: float, frame_index: int, species_index: int, pressure_index: int) -> None:
+        st = A.State(simulation_time, frame_index, species_index, pressure_index)
+        self._check(self._fn("set_state")(self._h, C.byref(st)))
+
+    def uniforms(self, dt: float = 1.0 / 60.0) -> np.ndarray:
+        out = (C.c_float * A.UNIFORM_FLOATS)()
+        self._check(self._fn("get_uniforms")(self._h, float(dt), out))
+        return np.frombuffer(out, dtype=np.float32).copy()
+
+    def snapshot(self) -> dict:
+        """All state needed to resume: counters plus the resident fields."""
+        snap = {"state": self.state}
+        for name in ("flow", "species", "pressure", "liquid", "reaction", "divergence"):
+            snap[name] = self.read(name)
+        return snap
+
+    def restore(self, snap: Mapping) -> None:
+        st = snap["state"]
+        self.set_state(st["simulation_time"], st["frame_index"], st["species_index"], st["pressure_index"])
+        for name in ("flow", "species", "pressure", "liquid", "reaction", "divergence"):
+            if name in snap:
+                self.write(name, snap[name])
+
+
+class FireXSim(_Handle):
+    """One simulation on the GPU through libfirex_b200.so."""
+
+    prefix = "firex_"
+
+    def __init__(self, dims: Iterable[int], options: A.Options | None = None, **kw):
+        super().__init__(load_library(), dims, options, **kw)
+
+    @property
+    def device_bytes(self) -> int:
+        v = C.c_uint64()
+        self._check(self._lib.firex_device_bytes(self._h, C.byref(v)))
+        return v.value
+
+    @property
+    def pressure_mode(self) -> int:
+        o = A.Options()
+        self._check(self._lib.firex_get_info(self._h, None, C.byref(o)))
+        return o.pressure_mode
+
+    @property
+    def stream(self) -> int:
+        return self._lib.firex_stream(self._h) or 0
+
+    def set_profiling(self, on: bool) -> None:
+        self._check(self._lib.firex_set_profiling(self._h, 1 if on else 0))
+
+    def pass_times(self) -> dict:
+        """Accumulated device ms and launch counts per pass since the previous call."""
+        ms = (C.c_double * len(A.PASS_NAMES))()
+        n = (C.c_int64 * len(A.PASS_NAMES))()
+        self._check(self._lib.firex_pass_times(self._h, ms, n))
+        return {name: (ms[i], n[i]) for i, name in enumerate(A.PASS_NAMES)}

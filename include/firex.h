@@ -1,0 +1,212 @@
+/*
+ * firex.h — C ABI of the B200-native Fire-X simulation step.
+ *
+ * The library owns all device memory; host buffers always belong to the caller.
+ * Every call returns an int status (FIREX_OK or a negative FIREX_ERR_*); the text of
+ * the most recent failure on a handle is available from firex_last_error().
+ * One simulation handle is not thread-safe: serialise calls on it (the reference
+ * engine serialises resource mutations on a promise queue, FireXEngine.ts:1882-1889).
+ *
+ * Reference interface replaced by this ABI (taesiri/Fire):
+ *   SimulationEngine          src/sim/types.ts:34-63
+ *   FireXEngine               src/sim/firex/FireXEngine.ts:370
+ * Each entry point below names the reference member it stands in for.
+ */
+#ifndef FIREX_H
+#define FIREX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIREX_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define FIREX_OK 0
+#define FIREX_ERR_BAD_ARG (-1)     /* invalid argument (reference: thrown Error / RangeError) */
+#define FIREX_ERR_OOM (-2)         /* device allocation failed; previous state kept */
+#define FIREX_ERR_BUDGET (-3)      /* admission refused by the memory budget / preflight */
+#define FIREX_ERR_CUDA (-4)        /* CUDA runtime error; the handle is poisoned */
+#define FIREX_ERR_TIMEOUT (-5)     /* a bounded device wait gave up */
+#define FIREX_ERR_UNSUPPORTED (-6) /* option combination not implemented */
+#define FIREX_ERR_STATE (-7)       /* handle disposed or poisoned (reference: device lost) */
+
+/* ---- options ---------------------------------------------------------------------- */
+/* Storage precision of the step. F32 mirrors the reference's f32 storage buffers;
+ * MIXED stores transported scalars (T, species) and the residual (correction) pressure
+ * in FP16 and keeps velocity, divergence and the primary pressure in FP32; all
+ * arithmetic is FP32. */
+#define FIREX_PRECISION_F32 0
+#define FIREX_PRECISION_MIXED 1
+
+/* Pressure branch (FireXEngine.ts:2175-2274). AUTO applies the reference rule: below
+ * FIREX_HEAVY_GRID_CELL_THRESHOLD cells the warm-started f32 global solve (branch A),
+ * at or above it the f16-storage tiled solve (branch B). */
+#define FIREX_PRESSURE_AUTO 0
+#define FIREX_PRESSURE_WARM_F32 1 /* branch A: f32, primary pressure warm-starts across steps */
+#define FIREX_PRESSURE_F16 2      /* branch B: f16 storage, f32 math, warm start */
+#define FIREX_PRESSURE_COLD_F32 3 /* branch C: f32, both solves cold-start in two shared buffers */
+
+#define FIREX_HEAVY_GRID_CELL_THRESHOLD (64LL * 1024 * 1024) /* gridConfiguration.ts:105 */
+
+/* Emitter model. BURNER is the reference's analytic elliptical burner
+ * (shaders.ts:101-133). SPHERES replaces it with a list of spheres in cell units:
+ * a cell is inside when |c + 0.5 - center|^2 <= radius^2 (float arithmetic, fixed
+ * order), and inside cells receive fuel = max(fuel, f*j), T = max(T, T_amb + (T_e -
+ * T_amb)*j) and the burner's swirl/lift with source = 1, where j is the per-step
+ * emission jitter. SPHERES is an extension (no reference counterpart). */
+#define FIREX_EMITTER_BURNER 0
+#define FIREX_EMITTER_SPHERES 1
+#define FIREX_MAX_SPHERES 8
+
+typedef struct firex_sphere {
+    float center[3];   /* cell units, x y z */
+    float radius;      /* cell units */
+    float fuel;        /* injected fuel concentration */
+    float temperature; /* injected temperature, K */
+} firex_sphere;
+
+typedef struct firex_options {
+    int32_t precision;             /* FIREX_PRECISION_* */
+    int32_t pressure_mode;         /* FIREX_PRESSURE_* */
+    int32_t pressure_iterations;   /* P, primary Jacobi sweeps per step */
+    int32_t correction_iterations; /* R, residual Jacobi sweeps per step */
+    int32_t emitter_mode;          /* FIREX_EMITTER_* */
+    int32_t num_spheres;           /* 0..FIREX_MAX_SPHERES */
+    firex_sphere spheres[FIREX_MAX_SPHERES];
+    uint64_t seed;                 /* seeds velocity noise and emission jitter */
+    float velocity_noise;          /* initial velocity: uniform in [-a, a] per component */
+    float emission_jitter;         /* per-step emission factor uniform in [1-a, 1+a] */
+    int32_t cinematic;             /* mixing.z; offline tiers force 1 (FireXEngine.ts:2097,2819) */
+    int32_t jacobi_block;          /* sweeps fused per Jacobi launch (temporal block); 0 = auto */
+    uint64_t memory_budget_bytes;  /* 0 = no budget; else create fails with FIREX_ERR_BUDGET */
+    int32_t reserved[8];
+} firex_options;
+
+/* Fills *opt with the defaults: F32, AUTO pressure, P = R = 64 (offline HD tier,
+ * FireXEngine.ts:240-252), burner emitter, seed 0, no noise, no jitter, cinematic 1. */
+void firex_default_options(firex_options* opt);
+
+/* ---- fields ----------------------------------------------------------------------- */
+/* Field ids for firex_read_field / firex_write_field. Layout is always the
+ * reference's: cell index = x + X*(y + Y*z) (shaders.ts:47-51), and the element types
+ * below, whatever the internal storage precision. */
+#define FIREX_FIELD_FLOW 0             /* float4 per cell: u v w T   (flow[0], canonical) */
+#define FIREX_FIELD_SPECIES 1          /* float4 per cell: fuel O2 products vapor (current) */
+#define FIREX_FIELD_PRESSURE 2         /* float per cell: current primary pressure */
+#define FIREX_FIELD_DIVERGENCE 3       /* float per cell: the divergence buffer */
+#define FIREX_FIELD_REACTION 4         /* float per cell: instantaneous reaction rate */
+#define FIREX_FIELD_LIQUID 5           /* uint32 per cell: deposited liquid, fixed point x4096 */
+#define FIREX_FIELD_EMITTER_MASK 6     /* uint8 per cell, read only: sphere emitter mask */
+#define FIREX_FIELD_CORRECTION 7       /* float per cell: last residual-pressure result */
+#define FIREX_FIELD_FINAL_DIVERGENCE 8 /* float per cell, read only: divergence of FLOW */
+#define FIREX_FIELD_COUNT 9
+
+/* Element size in bytes of a field (16, 4 or 1), or 0 for an unknown id. */
+size_t firex_field_element_size(int32_t field);
+
+/* ---- engine state ----------------------------------------------------------------- */
+typedef struct firex_state {
+    double simulation_time;  /* FireXEngine.simulationTime */
+    int64_t frame_index;     /* FireXEngine.frameIndex */
+    int32_t species_index;   /* FireXEngine.speciesIndex (0/1) */
+    int32_t pressure_index;  /* FireXEngine.pressureIndex (0/1) */
+} firex_state;
+
+#define FIREX_UNIFORM_FLOATS 44  /* FireXEngine.ts:163 */
+
+typedef struct firex_sim firex_sim;
+
+/* Allocates the solver bundle for a dims[0] x dims[1] x dims[2] grid and resets it.
+ * Axes must be positive multiples of 4 (gridConfiguration.ts:98, preflight :306-317).
+ * Replaces FireXEngine.initialize + createResourceSet (FireXEngine.ts:506-547,1536-1880).
+ * On failure *out is NULL; the message is available from firex_last_error(NULL). */
+int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** out);
+
+/* Releases every device allocation. Replaces FireXEngine.dispose (FireXEngine.ts:1034). */
+int firex_destroy(firex_sim* sim);
+
+/* Text of the last failure on sim (or of the last failed firex_create when sim is NULL). */
+const char* firex_last_error(const firex_sim* sim);
+
+/* Named engine parameter with the reference's clamps and fallbacks
+ * (FireXEngine.setParameter, FireXEngine.ts:937-1032). kind 0 passes a number, kind 1
+ * a boolean (value != 0). Unknown names are ignored, as in the reference. */
+#define FIREX_VALUE_NUMBER 0
+#define FIREX_VALUE_BOOLEAN 1
+int firex_set_parameter(firex_sim* sim, const char* name, int32_t kind, double value);
+int firex_get_parameter(const firex_sim* sim, const char* name, double* value);
+
+/* Re-initialises every field and the counters (FireXEngine.reset, FireXEngine.ts:843-852,
+ * initializeFields :1933-1974). */
+int firex_reset(firex_sim* sim);
+
+/* Advances nsteps fixed steps of dt seconds each (one encodeSimulationStep per step,
+ * FireXEngine.ts:2115-2276; simulationTime += dt and frameIndex += 1 per step as in
+ * renderOfflineFrameInternal, :669-682). dt is a double like the reference's JS number:
+ * simulationTime accumulates in double and the uniform block holds its f32 rounding.
+ * Asynchronous: returns once the work is queued. */
+int firex_step(firex_sim* sim, int32_t nsteps, double dt);
+
+/* Blocks until queued work has finished (FireXEngine: queue.onSubmittedWorkDone, :692). */
+int firex_sync(firex_sim* sim);
+
+/* Copies a whole field to / from caller memory in the reference layout. bytes must equal
+ * cells * firex_field_element_size(field). Synchronous. (No reference counterpart: the
+ * reference never reads fields back; this is the field-readback half of the drop-in.) */
+int firex_read_field(firex_sim* sim, int32_t field, void* host, size_t bytes);
+int firex_write_field(firex_sim* sim, int32_t field, const void* host, size_t bytes);
+
+/* Post-projection divergence of FLOW over interior cells (the one-cell outer shell is
+ * excluded, qualityShaders.ts:47-57), reduced in FP64: out[0] = L2 norm, out[1] = max
+ * abs, out[2] = number of interior cells. (Presentation diagnostic, FireXEngine.ts:2588-2596.) */
+int firex_divergence_norm(firex_sim* sim, double out[3]);
+
+/* Counters that decide ping-pong parity and time (FireXEngine.ts:396-409). */
+int firex_get_state(const firex_sim* sim, firex_state* st);
+int firex_set_state(firex_sim* sim, const firex_state* st);
+
+/* The 44-float uniform block the next step will use for time dt (writeUniforms,
+ * FireXEngine.ts:2043-2113). */
+int firex_get_uniforms(const firex_sim* sim, double dt, float out[FIREX_UNIFORM_FLOATS]);
+
+/* Grid dimensions and options the handle was created with. */
+int firex_get_info(const firex_sim* sim, int32_t dims[3], firex_options* opt);
+
+/* Device bytes held by the handle (actual allocation, not the reference's model). */
+int firex_device_bytes(const firex_sim* sim, uint64_t* bytes);
+
+/* The reference's persistent-memory model (estimateFireXGridMemory,
+ * gridConfiguration.ts:272-291): 116 B/cell below the heavy threshold, 108 B/cell at
+ * or above, + 80 B/particle + the 64^3 RGBA8 detail texture. */
+uint64_t firex_reference_memory_estimate(const int32_t dims[3], int64_t particle_count);
+
+/* CUDA stream the handle runs on (cudaStream_t as void*), for callers that order their
+ * own work after a step. */
+void* firex_stream(const firex_sim* sim);
+
+/* ---- profiling (reference: per-pass encoder labels and CPU phase timers,
+ * FireXEngine.ts:712-797; here CUDA events on the handle's stream) ------------------- */
+#define FIREX_PASS_SIMULATE 0   /* advect/react (simulate) */
+#define FIREX_PASS_DIVERGENCE 1 /* both divergence passes */
+#define FIREX_PASS_JACOBI 2     /* every primary and residual Jacobi launch */
+#define FIREX_PASS_PROJECT 3    /* both projections */
+#define FIREX_PASS_OTHER 4      /* parameter upload and buffer clears */
+#define FIREX_PASS_COUNT 5
+
+/* Turns per-pass event recording on (1) or off (0) for subsequent steps. */
+int firex_set_profiling(firex_sim* sim, int32_t on);
+
+/* Waits for the stream, then returns and clears the accumulated device milliseconds per
+ * pass (ms[FIREX_PASS_COUNT]) and the number of kernel launches per pass
+ * (launches[FIREX_PASS_COUNT]) since the previous call. Either pointer may be NULL. */
+int firex_pass_times(firex_sim* sim, double* ms, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FIREX_H */
