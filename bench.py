@@ -219,9 +219,8 @@ def run_gpu(args) -> None:
     sim.step(args.warmup, DT)
     sim.sync()
 
-    # ---- device-resident timed region ----
-    sim.set_profiling(True)
-    sim.pass_times()  # clear
+    # ---- device-resident timed region (each step replays the captured CUDA graph) ----
+    sim.pass_times()  # clear the launch counters
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     barrier()
     torch.cuda.synchronize()
@@ -235,10 +234,19 @@ def run_gpu(args) -> None:
     barrier()
     step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     total_ms = evs[0].elapsed_time(evs[-1])
-    passes = sim.pass_times()
-    sim.set_profiling(False)
+    launches = sum(n for _, n in sim.pass_times().values())
     total_ms_max = max_over_ranks(total_ms)
     value = n_cells * args.steps * world / (total_ms_max / 1e3) / 1e9
+
+    # ---- per-pass device times: the same steps launched pass by pass with CUDA events
+    # recorded on the simulation's stream between passes (a graph hides its nodes) ----
+    prof_steps = max(3, min(args.steps, 20))
+    sim.set_profiling(True)
+    sim.pass_times()
+    barrier()
+    sim.step(prof_steps, DT)
+    passes = sim.pass_times()
+    sim.set_profiling(False)
 
     # ---- end-to-end through the C ABI with host buffers ----
     pinned = torch.empty((DIMS[2], DIMS[1], DIMS[0], 4), dtype=torch.float32, pin_memory=True)
@@ -268,7 +276,6 @@ def run_gpu(args) -> None:
             traffic = json.loads(tp.read_text()).get("bytes_per_launch_hd")
         except Exception:
             traffic = None
-    launches = sum(n for _, n in passes.values())
 
     if rank == 0:
         cpu = None
@@ -287,7 +294,8 @@ def run_gpu(args) -> None:
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "traffic": traffic, "bytes_per_cell": JACOBI_BYTES_PER_CELL, "avg_launch_us": jac_avg_ms * 1e3,
                          "launches": jac_n},
-            "passes_ms_per_step": {k: v[0] / args.steps for k, v in passes.items()},
+            "passes_ms_per_step": {k: v[0] / prof_steps for k, v in passes.items()},
+            "profiled_steps": prof_steps,
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

@@ -10,7 +10,7 @@ from ._abi import (  # noqa: F401
     EMITTER_BURNER, EMITTER_SPHERES, FIELD_NAMES, PRECISION_F32, PRECISION_MIXED, PRESSURE_AUTO,
     PRESSURE_COLD_F32, PRESSURE_F16, PRESSURE_WARM_F32,
 )
-from .sim import FireXError, FireXSim, load_library, make_options  # noqa: F401
+from .sim import FireXBatch, FireXError, FireXSim, load_library, make_options, planned_device_bytes  # noqa: F401
 from .engine import FireXEngine  # noqa: F401
 
-__all__ = ["FireXEngine", "FireXSim", "FireXError", "make_options", "load_library"]
+__all__ = ["FireXEngine", "FireXSim", "FireXBatch", "FireXError", "make_options", "load_library", "planned_device_bytes"]

@@ -43,6 +43,11 @@ FIELD_CORRECTION = 7
 FIELD_FINAL_DIVERGENCE = 8
 FIELD_COUNT = 9
 
+JACOBI_AUTO = 0
+JACOBI_UNBLOCKED = 1
+JACOBI_ZMARCH = 2
+JACOBI_FUSED = 3
+
 VALUE_NUMBER = 0
 VALUE_BOOLEAN = 1
 
@@ -98,7 +103,19 @@ class Options(C.Structure):
         ("cinematic", C.c_int32),
         ("jacobi_block", C.c_int32),
         ("memory_budget_bytes", C.c_uint64),
-        ("reserved", C.c_int32 * 8),
+        ("jacobi_zchunk", C.c_int32),
+        ("reserved", C.c_int32 * 7),
+    ]
+
+
+class Diagnostics(C.Structure):
+    _fields_ = [
+        ("fast_division", C.c_int32),
+        ("jacobi_block", C.c_int32),
+        ("jacobi_zchunk", C.c_int32),
+        ("graph", C.c_int32),
+        ("launches_per_step", C.c_int32),
+        ("reserved", C.c_int32 * 11),
     ]
 
 
@@ -140,6 +157,20 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_stream": (vp, [vp]),
         "firex_set_profiling": (C.c_int, [vp, C.c_int32]),
         "firex_pass_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
+        "firex_planned_device_bytes": (C.c_uint64, [DIMS, C.POINTER(Options)]),
+        "firex_set_graphs": (C.c_int, [vp, C.c_int32]),
+        "firex_set_jacobi": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
+        "firex_get_diagnostics": (C.c_int, [vp, C.POINTER(Diagnostics)]),
+        "firex_batch_set_jacobi": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
+        "firex_batch_create": (C.c_int, [C.POINTER(vp)]),
+        "firex_batch_destroy": (C.c_int, [vp]),
+        "firex_batch_add": (C.c_int, [vp, vp]),
+        "firex_batch_remove": (C.c_int, [vp, vp]),
+        "firex_batch_size": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+        "firex_batch_step": (C.c_int, [vp, C.c_int32, C.c_double]),
+        "firex_batch_sync": (C.c_int, [vp]),
+        "firex_batch_last_error": (C.c_char_p, [vp]),
+        "firex_batch_stream": (vp, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -154,6 +185,9 @@ HEADER_SYMBOLS = [
     "firex_sync", "firex_read_field", "firex_write_field", "firex_divergence_norm", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_stream", "firex_set_profiling", "firex_pass_times",
+    "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_batch_create", "firex_batch_destroy",
+    "firex_batch_add", "firex_batch_remove", "firex_batch_size", "firex_batch_step", "firex_batch_sync",
+    "firex_batch_last_error", "firex_batch_stream",
 ]
 
 PASS_NAMES = ("simulate", "divergence", "jacobi", "project", "other")

@@ -102,3 +102,74 @@ FXD float fx_velocity_noise(uint64_t seed, uint64_t cell, int comp, float a) {
     float u = __fmul_rn((float)(h >> 40), 1.0f / 16777216.0f);
     return __fmul_rn(a, __fsub_rn(__fmul_rn(2.0f, u), 1.0f));
 }
+
+// ---------------------------------------------------------------------------------------
+// Device-resident simulation descriptor. Parities and counters live on the device and
+// are advanced by the step epilogue kernel, so a whole step (or a batch of simulations
+// stepping together) is a fixed sequence of launches that a CUDA graph can replay with
+// no per-step host arguments. The host keeps a mirror of the same counters, advanced
+// by the same rules, for reads between steps.
+enum FxStorage { FX_STORAGE_F32 = 0, FX_STORAGE_MIXED = 1 };
+
+struct __align__(16) FxSimDev {
+    FxParams prm;          // parameters of the running step (time fields set by step_begin)
+    int X, Y, Z;
+    int P, R;              // primary / residual Jacobi sweeps per step
+    int mode;              // FIREX_PRESSURE_WARM_F32 / _F16 / _COLD_F32 (resolved)
+    int storage;           // FxStorage
+    int active;            // 0: skipped by every kernel (batch slot parked)
+    int fi, si, pi;        // flow, species, pressure parity at the start of the step
+    int pad0;
+    double simTime;        // FireXEngine.simulationTime
+    double dt;             // dt of the next step
+    long long frame;       // FireXEngine.frameIndex
+    uint64_t seed;
+    float jitterAmp;
+    int pad1;
+    float metric[4];       // grid / domainExtent (shaders.ts:39-41), host-computed in f32
+    float jc[4];           // Jacobi wx, wy, wz, 2(wx+wy+wz) (shaders.ts:386-389), f32
+    float jcRcp;           // RN(1 / jc[3])
+    int jcFastDiv;         // 1: x / jc[3] may use fx_div_by_const (checked exhaustively)
+    int pad2[2];
+    void* flow[2];         // float4 records (both storages)
+    void* species[2];      // float4 (F32) or 4 x half (MIXED)
+    void* p[2];            // primary pressure: float (F32 / COLD) or half (F16 / MIXED)
+    void* corr[2];         // residual pressure (aliases p[] in branch C)
+    float* div;
+    float* reaction;
+    uint32_t* liquid;
+};
+
+// Work decomposition shared by every batched pass: each pass walks a flat list of
+// bricks across all simulations of a batch; start[shape][s] is the first brick of
+// simulation s (prefix sums over the batch), so one launch covers uneven grids.
+#define FX_MAX_BATCH 512
+enum FxShape { FX_SHAPE_CELL = 0, FX_SHAPE_ROW4 = 1, FX_SHAPE_COL = 2, FX_SHAPE_ZM = 3, FX_NSHAPES = 4 };
+// CELL: 32 x 4 x 2 cells, one thread per cell (simulate).
+// ROW4: 256 groups of 4 consecutive x cells in memory order (stencils).
+// COL : column tiles of the temporally blocked Jacobi (see fx_jacobi_tb.cuh).
+// ZM  : z-marching tiles of the single-sweep Jacobi (see fx_jacobi_zm.cuh).
+#define FX_CELL_BX 32
+#define FX_CELL_BY 4
+#define FX_CELL_BZ 2
+#define FX_ROW4_THREADS 256
+
+struct FxBatchDev {
+    int nsims;
+    int pad;
+    int total[FX_NSHAPES];
+    int colTileX, colTileY;        // interior tile of the COL shape
+    FxSimDev* sims[FX_MAX_BATCH];
+    int start[FX_NSHAPES][FX_MAX_BATCH + 1];
+};
+
+// Finds the simulation owning brick w (start[] ascending, start[nsims] = total).
+FXD int fx_find_sim(const int* __restrict__ start, int nsims, int w) {
+    int lo = 0, hi = nsims - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(start + mid) <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}

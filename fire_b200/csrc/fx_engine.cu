@@ -1,21 +1,28 @@
-// fx_engine.cpp — the Fire-X engine behind the C ABI (include/firex.h).
+// fx_engine.cu — the Fire-X engine behind the C ABI (include/firex.h).
 //
 // Host-side counterpart of FireXEngine (src/sim/firex/FireXEngine.ts): named parameters
-// with the reference's clamps, the 44-float uniform block, resource allocation with
-// transactional failure, reset, and the per-step dispatch graph with its ping-pong
-// parity and pressure branches. All device work is queued on the handle's own stream.
+// with the reference's clamps, the 44-float uniform block, transactional allocation,
+// reset, and the per-step dispatch graph with its ping-pong parities and pressure
+// branches. Each simulation owns a device descriptor (FxSimDev); a standalone simulation
+// steps as a batch of one, and firex_batch_* steps many simulations through the same
+// launches. A step is captured once into a CUDA graph and replayed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/firex.h"
 #include "fx_internal.h"
+#include "fx_jacobi_tb.cuh"
+#include "fx_jacobi_zm.cuh"
 
 namespace {
 
@@ -86,52 +93,371 @@ struct DeviceGuard {
     }
 };
 
+// Seeded per-step emission factor in [1-a, 1+a] (extension); same operations as the
+// step prologue kernel.
+float host_jitter(uint64_t seed, int64_t f, float a) {
+    auto mix = [](uint64_t z) {
+        z += 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    uint64_t h = mix(mix(seed ^ 0xBB67AE8584CAA73Bull) + (uint64_t)f);
+    float u = (float)(h >> 40) * (1.0f / 16777216.0f);
+    return 1.0f + a * (2.0f * u - 1.0f);
+}
+
+long long bricks_cell(int X, int Y, int Z) {
+    return (long long)((X + FX_CELL_BX - 1) / FX_CELL_BX) * ((Y + FX_CELL_BY - 1) / FX_CELL_BY) *
+           ((Z + FX_CELL_BZ - 1) / FX_CELL_BZ);
+}
+long long bricks_row4(int X, int Y, int Z) {
+    long long groups = (long long)(X / 4) * Y * Z;
+    return (groups + FX_ROW4_THREADS - 1) / FX_ROW4_THREADS;
+}
+
+// The host-side mirror of a step graph's launch sequence and its cache key.
+struct StepPlan {
+    int storage = 0;
+    bool half = false;
+    int pmode = FX_TB_F32;    // pressure storage / rounding of the fused Jacobi
+    int maxP = 0, maxR = 0;
+    int k = 1, zc = 16;       // fused sweeps per Jacobi launch, z planes per CTA
+    int zmZc = 16;            // z planes per CTA of the single-sweep (z-marching) kernel
+    bool row4 = false;        // single sweeps by the unblocked kernel instead
+    bool fuseP = false, fuseR = false;
+    int bricks[FX_NSHAPES] = {0, 0, 0, 0};
+    auto key() const {
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, bricks[0], bricks[1], bricks[2],
+                        bricks[3]);
+    }
+    bool operator<(const StepPlan& o) const { return key() < o.key(); }
+};
+
+// A phase of n sweeps may fuse k sweeps per launch when every member runs the same n
+// and the launch count (n/k fused + n%k single) has the parity of n: the result then
+// lands in the buffer the reference's ping-pong leaves it in.
+bool can_fuse(int k, int n) { return k > 1 && n >= k && ((k - 1) * (n / k)) % 2 == 0; }
+
+int jacobi_phase_launches(const StepPlan& pl, int phase) {
+    const int n = phase == 0 ? pl.maxP : pl.maxR;
+    const bool fuse = phase == 0 ? pl.fuseP : pl.fuseR;
+    return fuse ? n / pl.k + n % pl.k : n;
+}
+
+void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, int phase) {
+    const int n = phase == 0 ? pl.maxP : pl.maxR;
+    const bool fuse = phase == 0 ? pl.fuseP : pl.fuseR;
+    int launch = 0, sweep = 0;
+    if (fuse) {
+        for (; sweep + pl.k <= n; sweep += pl.k, ++launch)
+            fx_launch_jacobi_tb(st, pl.pmode, pl.k, B, pl.bricks[FX_SHAPE_COL], phase, launch, pl.zc);
+    }
+    for (; sweep < n; ++sweep, ++launch) {
+        if (pl.row4) fx_launch_jacobi(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], phase, launch, sweep);
+        else fx_launch_jacobi_zm(st, pl.half, B, pl.bricks[FX_SHAPE_ZM], phase, launch, sweep, pl.zmZc);
+    }
+}
+
+void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
+    fx_launch_step_begin(st, B);
+    fx_launch_simulate(st, pl.storage, B, pl.bricks[FX_SHAPE_CELL]);
+    fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 0);
+    enqueue_jacobi_phase(st, pl, B, 0);
+    fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 0);
+    fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 1);
+    enqueue_jacobi_phase(st, pl, B, 1);
+    fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 1);
+    fx_launch_step_end(st, B);
+}
+
+// Jacobi kernel when the caller did not choose one (measured on B200, 96+96 sweeps):
+// below 16 Mi cells per batch the unblocked kernel wins (the data stays in L2 and more
+// CTAs hide latency); above it the z-marching kernel with 32-plane chunks reaches 85-90 %
+// of the measured HBM copy bandwidth. fire_b200/autotune.py refines this per workload.
+void default_jacobi(long long cells, int* kernel, int* zc) {
+    *kernel = cells >= (16LL << 20) ? FIREX_JACOBI_ZMARCH : FIREX_JACOBI_UNBLOCKED;
+    *zc = 32;
+}
+
+// z chunk of the z-marching kernel when not chosen: the largest of 32, 16, 8 planes that
+// still yields three CTAs per SM over the batch.
+int zm_chunk(long long tiles32, long long tiles16) {
+    return tiles32 >= 3LL * 148 ? 32 : (tiles16 >= 3LL * 148 ? 16 : 8);
+}
+
 }  // namespace
 
+struct firex_batch;
+
+// Whether fx_div_by_const(x, d, rcp) equals IEEE x / d for every finite float x on this
+// device, checked once per (device, d) by fxk_check_div (about a millisecond). Results
+// are cached for the life of the process. Any CUDA error answers "no".
+static bool fast_division_ok(int device, float d, float rcp) {
+    static std::map<std::pair<int, uint32_t>, bool> cache;
+    uint32_t bits;
+    std::memcpy(&bits, &d, 4);
+    auto key = std::make_pair(device, bits);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    bool ok = false;
+    unsigned long long* dcount = nullptr;
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaMalloc(&dcount, sizeof(unsigned long long)) == cudaSuccess &&
+        cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), st) == cudaSuccess) {
+        fx_launch_check_div(st, d, rcp, dcount);
+        unsigned long long bad = ~0ull;
+        if (cudaMemcpyAsync(&bad, dcount, sizeof(bad), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
+            cudaStreamSynchronize(st) == cudaSuccess)
+            ok = bad == 0;
+    }
+    cudaGetLastError();
+    if (dcount) cudaFree(dcount);
+    if (st) cudaStreamDestroy(st);
+    cache[key] = ok;
+    return ok;
+}
+
+// ---- one simulation ------------------------------------------------------------------------
 struct firex_sim {
     int X = 0, Y = 0, Z = 0;
     long long N = 0;
     firex_options opt{};
     int mode = FIREX_PRESSURE_WARM_F32;
+    int storage = FX_STORAGE_F32;
+    bool half = false;  // pressure storage is FP16
     int device = 0;
     double named[kNumParams];
+    int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;
 
-    double simTime = 0;
-    int64_t frame = 0;
-    int speciesIndex = 0, pressureIndex = 0;
-    int lastCorrection = 0;
-    bool lastCorrectionShared = false;
+    FxSimDev h{};           // host mirror of the device descriptor
+    FxSimDev* d = nullptr;  // device descriptor
+    bool dirty = true;      // host mirror has changes the device has not seen
 
-    cudaStream_t stream = nullptr;
+    cudaStream_t own = nullptr;
+    firex_batch* batch = nullptr;  // set while a member of a batch
+    firex_batch* solo = nullptr;   // the one-member batch used for standalone steps
+
     std::vector<void*> allocations;
     size_t bytes = 0;
-    float4* flow[2] = {nullptr, nullptr};
-    float4* species[2] = {nullptr, nullptr};
-    float* pressure[2] = {nullptr, nullptr};
-    float* correction[2] = {nullptr, nullptr};
-    float* div = nullptr;
-    float* reaction = nullptr;
-    uint32_t* liquid = nullptr;
-    FxParams* d_params = nullptr;
-    double* d_partial = nullptr;
+    void* d_tmp = nullptr;          // 4 B/cell scratch: emitter mask, final divergence
+    double* d_partial = nullptr;    // divergence-norm partials
     double* d_norm = nullptr;
-    float* d_tmp = nullptr;
-
     std::string err;
     bool poisoned = false;
 
-    // Per-pass profiling: an event is recorded at every pass boundary; the elapsed time
-    // between consecutive events is charged to the pass that ran between them.
+    cudaStream_t stream() const;
+
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        poisoned = true;
+        err = std::string(what) + ": " + cudaGetErrorString(e);
+        return FIREX_ERR_CUDA;
+    }
+
+    void* alloc(size_t nbytes) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, nbytes ? nbytes : 1) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        allocations.push_back(p);
+        bytes += nbytes;
+        return p;
+    }
+
+    static size_t planned_bytes(long long N, int storage, int mode) {
+        const size_t species = storage == FX_STORAGE_MIXED ? 8 : 16;
+        const size_t pbytes = (storage == FX_STORAGE_MIXED || mode == FIREX_PRESSURE_F16) ? 2 : 4;
+        const size_t npress = mode == FIREX_PRESSURE_COLD_F32 ? 2 : 4;
+        const size_t per = 16 * 2 + species * 2 + pbytes * npress + 4 /*div*/ + 4 /*reaction*/ + 4 /*liquid*/ + 4 /*tmp*/;
+        return (size_t)N * per + sizeof(FxSimDev) + 64 * 1024;
+    }
+
+    size_t species_bytes() const { return storage == FX_STORAGE_MIXED ? 8 : 16; }
+    size_t pressure_bytes() const { return half ? 2 : 4; }
+
+    // writeUniforms (FireXEngine.ts:2043-2113); the time fields are rewritten on the
+    // device at the start of every step from the counters.
+    void build_params(FxParams& p, double dt) const {
+        std::memset(&p, 0, sizeof(p));
+        auto P = [&](const char* n) { return named[param_slot(n)]; };
+        const double cells = (double)X * (double)Y * (double)Z;
+        const double u[FIREX_UNIFORM_FLOATS] = {
+            (double)X, (double)Y, (double)Z, cells,
+            dt, h.simTime, (double)h.frame, dt,
+            P("fuelRate"), P("oxygenRate"), P("heatEfficiency"), P("vorticity"),
+            P("waterFlow"), (P("sprayAngle") * M_PI) / 180, P("waterEnabled") != 0 ? 1.0 : 0.0, 300,
+            P("cameraYaw"), P("cameraPitch"), P("cameraDistance"), 1,  // canvas aspect (presentation only)
+            1, 1, 0, 0,                                                // canvas size, rays, particles
+            P("viewMode"), P("aimHeight"), P("nozzleType"), P("exposure"),
+            P("burnerSize"), P("burnerDepth"), P("sourceThickness"), P("firePower"),
+            P("domainWidth"), P("domainHeight"), P("domainDepth"), 0,
+            P("sourceLift"), P("buoyancyScale"), P("flamePersistence"), P("viewZoom"),
+            P("airEntrainment"), P("frontDefinition"), opt.cinematic ? 1.0 : 0.0, P("opticalDetailTarget")};
+        for (int i = 0; i < FIREX_UNIFORM_FLOATS; ++i) p.u[i] = (float)u[i];
+        p.emitter_mode = opt.emitter_mode;
+        p.num_spheres = opt.emitter_mode == FIREX_EMITTER_SPHERES ? opt.num_spheres : 0;
+        for (int s = 0; s < FIREX_MAX_SPHERES; ++s) p.spheres[s] = opt.spheres[s];
+        p.jitter = host_jitter(opt.seed, h.frame, opt.emission_jitter);
+    }
+
+    // Stencil constants in f32, the same operations as cellMetric() and the Jacobi
+    // weights of shaders.ts:39-41,386-389 (IEEE single precision on the host).
+    void refresh_params() {
+        build_params(h.prm, h.dt);
+        const float* u = h.prm.u;
+        const float ex = std::max(u[32], 0.001f), ey = std::max(u[33], 0.001f), ez = std::max(u[34], 0.001f);
+        h.metric[0] = u[0] / ex;
+        h.metric[1] = u[1] / ey;
+        h.metric[2] = u[2] / ez;
+        h.metric[3] = 0.0f;
+        h.jc[0] = h.metric[0] * h.metric[0];
+        h.jc[1] = h.metric[1] * h.metric[1];
+        h.jc[2] = h.metric[2] * h.metric[2];
+        h.jc[3] = 2.0f * (h.jc[0] + h.jc[1] + h.jc[2]);
+        h.jcRcp = 1.0f / h.jc[3];
+        h.jcFastDiv = fast_division_ok(device, h.jc[3], h.jcRcp) ? 1 : 0;
+        dirty = true;
+    }
+
+    // Uploads the host mirror when it changed (parameters, dt, counters set by the caller).
+    void flush(cudaStream_t st) {
+        if (!dirty) return;
+        fx_launch_upload_desc(st, h, d);
+        dirty = false;
+    }
+
+    // Advances the host mirror exactly as fxk_step_end advances the device.
+    void advance_mirror() {
+        h.simTime = h.simTime + h.dt;
+        h.frame += 1;
+        h.fi ^= 1;
+        h.si ^= 1;
+        h.pi = (h.mode == FIREX_PRESSURE_COLD_F32) ? (h.P & 1) : (h.pi ^ (h.P & 1));
+    }
+
+    int reset();
+    void release();
+};
+
+// ---- a batch of simulations stepping together ------------------------------------------------
+struct firex_batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<firex_sim*> members;
+    FxBatchDev* d = nullptr;
+    FxBatchDev* h = nullptr;  // host copy of the table
+    bool tableDirty = true;
+    std::map<StepPlan, cudaGraphExec_t> graphs;
+    bool useGraphs = true;
     bool profiling = false;
+    bool isSolo = false;
+    StepPlan last{};                 // plan of the most recent step (diagnostics)
+    bool lastGraph = false;
+    int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;  // batch override (AUTO: first member's)
+    int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
+    std::string err;
+
+    // per-pass profiling (events between passes; graphs are bypassed while profiling)
     std::vector<cudaEvent_t> evPool;
-    std::vector<std::pair<cudaEvent_t, int>> evMarks;  // (event, pass that ends here)
+    std::vector<std::pair<cudaEvent_t, int>> evMarks;
     size_t evUsed = 0;
     double passMs[FIREX_PASS_COUNT] = {0};
     int64_t passLaunches[FIREX_PASS_COUNT] = {0};
     int64_t pendingLaunches[FIREX_PASS_COUNT] = {0};
 
+    int fail(int code, const std::string& msg) {
+        err = msg;
+        return code;
+    }
+
+    void rebuild_table() {
+        std::memset(h, 0, sizeof(FxBatchDev));
+        h->nsims = (int)members.size();
+        tableK = -1;
+        tableDirty = true;
+    }
+
+    // Fills the brick prefix sums for the launch shape (k, zc).
+    void fill_table(int k, int zc, int zmZc) {
+        int acc[FX_NSHAPES] = {0, 0, 0, 0};
+        h->nsims = (int)members.size();
+        for (size_t i = 0; i < members.size(); ++i) {
+            firex_sim* s = members[i];
+            h->sims[i] = s->d;
+            h->start[FX_SHAPE_CELL][i] = acc[FX_SHAPE_CELL];
+            h->start[FX_SHAPE_ROW4][i] = acc[FX_SHAPE_ROW4];
+            h->start[FX_SHAPE_COL][i] = acc[FX_SHAPE_COL];
+            h->start[FX_SHAPE_ZM][i] = acc[FX_SHAPE_ZM];
+            acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z);
+            acc[FX_SHAPE_ROW4] += (int)bricks_row4(s->X, s->Y, s->Z);
+            acc[FX_SHAPE_COL] += k > 1 ? fx_tb_bricks(s->X, s->Y, s->Z, k, zc) : 0;
+            acc[FX_SHAPE_ZM] += fx_zm_bricks(s->X, s->Y, s->Z, zmZc);
+        }
+        for (int j = 0; j < FX_NSHAPES; ++j) {
+            h->start[j][members.size()] = acc[j];
+            h->total[j] = acc[j];
+        }
+        tableK = k;
+        tableZc = zc;
+        tableZmZc = zmZc;
+        tableDirty = true;
+    }
+
+    StepPlan plan() {
+        StepPlan p;
+        if (members.empty()) return p;
+        p.storage = members[0]->storage;
+        p.half = members[0]->half;
+        p.pmode = !p.half ? FX_TB_F32 : (p.storage == FX_STORAGE_F32 ? FX_TB_F16_ROUND : FX_TB_F16);
+        bool uniformP = true, uniformR = true;
+        long long cells = 0;
+        for (firex_sim* s : members) {
+            p.maxP = std::max(p.maxP, s->h.P);
+            p.maxR = std::max(p.maxR, s->h.R);
+            uniformP = uniformP && s->h.P == members[0]->h.P;
+            uniformR = uniformR && s->h.R == members[0]->h.R;
+            cells += s->N;
+        }
+        const bool own = jacobiKernel != FIREX_JACOBI_AUTO;
+        int kernel = own ? jacobiKernel : members[0]->jacobiKernel;
+        int k = own ? jacobiK : members[0]->jacobiK;
+        int zc = own ? jacobiZc : members[0]->jacobiZc;
+        int dzc = 32;
+        if (kernel == FIREX_JACOBI_AUTO) default_jacobi(cells, &kernel, &dzc);
+        if (kernel != FIREX_JACOBI_FUSED || (k != 2 && k != 3 && k != 4 && k != 6)) k = 1;
+        long long zm32 = 0, zm16 = 0;
+        for (firex_sim* s : members) {
+            zm32 += fx_zm_bricks(s->X, s->Y, s->Z, 32);
+            zm16 += fx_zm_bricks(s->X, s->Y, s->Z, 16);
+        }
+        p.k = k;
+        p.zc = zc > 0 ? zc : 16;
+        p.fuseP = uniformP && can_fuse(k, p.maxP);
+        p.fuseR = uniformR && can_fuse(k, p.maxR);
+        if (!p.fuseP && !p.fuseR) p.k = 1;
+        p.row4 = kernel == FIREX_JACOBI_UNBLOCKED;
+        p.zmZc = (kernel == FIREX_JACOBI_ZMARCH && zc > 0) ? zc : zm_chunk(zm32, zm16);
+        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc) fill_table(p.k, p.zc, p.zmZc);
+        for (int j = 0; j < FX_NSHAPES; ++j) p.bricks[j] = h->total[j];
+        return p;
+    }
+
+    cudaError_t flush_table() {
+        if (!tableDirty) return cudaSuccess;
+        cudaError_t e = cudaMemcpyAsync(d, h, sizeof(FxBatchDev), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // h may change right after
+        tableDirty = false;
+        return e;
+    }
+
     void mark(int pass, int launches) {
-        pendingLaunches[pass] += launches;
+        if (pass >= 0) pendingLaunches[pass] += launches;
         if (!profiling) return;
         if (evUsed == evPool.size()) {
             cudaEvent_t e;
@@ -142,20 +468,10 @@ struct firex_sim {
         cudaEventRecord(e, stream);
         evMarks.emplace_back(e, pass);
     }
-    void begin_marks() {
-        if (!profiling) return;
-        if (evUsed == evPool.size()) {
-            cudaEvent_t e;
-            cudaEventCreate(&e);
-            evPool.push_back(e);
-        }
-        cudaEvent_t e = evPool[evUsed++];
-        cudaEventRecord(e, stream);
-        evMarks.emplace_back(e, -1);
-    }
+
     int collect_marks() {
-        cudaError_t err = cudaStreamSynchronize(stream);
-        if (err != cudaSuccess) return cuda_fail(err, "pass_times");
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return fail(FIREX_ERR_CUDA, std::string("pass_times: ") + cudaGetErrorString(e));
         for (size_t i = 1; i < evMarks.size(); ++i) {
             if (evMarks[i].second < 0) continue;
             float ms = 0;
@@ -171,164 +487,196 @@ struct firex_sim {
         return FIREX_OK;
     }
 
-    FxGrid grid() const { return FxGrid{X, Y, Z}; }
-
-    int fail(int code, const std::string& msg) {
-        err = msg;
-        return code;
+    // One step of every member with per-pass event marks (no graph).
+    void enqueue_profiled(const StepPlan& pl) {
+        mark(-1, 0);
+        fx_launch_step_begin(stream, d);
+        mark(FIREX_PASS_OTHER, 1);
+        fx_launch_simulate(stream, pl.storage, d, pl.bricks[FX_SHAPE_CELL]);
+        mark(FIREX_PASS_SIMULATE, 1);
+        fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 0);
+        mark(FIREX_PASS_DIVERGENCE, 1);
+        enqueue_jacobi_phase(stream, pl, d, 0);
+        mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 0));
+        fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 0);
+        mark(FIREX_PASS_PROJECT, 1);
+        fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 1);
+        mark(FIREX_PASS_DIVERGENCE, 1);
+        enqueue_jacobi_phase(stream, pl, d, 1);
+        mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 1));
+        fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 1);
+        mark(FIREX_PASS_PROJECT, 1);
+        fx_launch_step_end(stream, d);
+        mark(FIREX_PASS_OTHER, 1);
     }
-    int cuda_fail(cudaError_t e, const char* what) {
-        poisoned = true;
-        err = std::string(what) + ": " + cudaGetErrorString(e);
-        return FIREX_ERR_CUDA;
-    }
 
-    template <typename T>
-    T* alloc(size_t n) {
-        if (n == 0) n = 1;
-        void* p = nullptr;
-        if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
+    cudaError_t graph_for(const StepPlan& pl, cudaGraphExec_t* out) {
+        auto it = graphs.find(pl);
+        if (it != graphs.end()) {
+            *out = it->second;
+            return cudaSuccess;
         }
-        allocations.push_back(p);
-        bytes += n * sizeof(T);
-        return static_cast<T*>(p);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        enqueue_step_launches(stream, pl, d);
+        e = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) return e;
+        cudaGraphExec_t ex = nullptr;
+        e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return e;
+        graphs[pl] = ex;
+        *out = ex;
+        return cudaSuccess;
     }
 
-    void release() {
+    int step(int nsteps, double dt) {
+        if (members.empty() || nsteps == 0) return FIREX_OK;
+        DeviceGuard dg(device);
+        for (firex_sim* s : members) {
+            if (s->poisoned) return fail(FIREX_ERR_STATE, "a member simulation is poisoned");
+            if (s->h.dt != dt) {
+                s->h.dt = dt;
+                s->refresh_params();
+            }
+            s->flush(stream);
+        }
+        const StepPlan pl = plan();
+        cudaError_t e = flush_table();
+        if (e != cudaSuccess) return poison(e, "batch table");
+        cudaGraphExec_t ex = nullptr;
+        if (useGraphs && !profiling) {
+            e = graph_for(pl, &ex);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                useGraphs = false;  // direct launches remain correct
+            }
+        }
+        last = pl;
+        lastGraph = ex != nullptr;
+        for (int i = 0; i < nsteps; ++i) {
+            if (profiling) enqueue_profiled(pl);
+            else if (ex) e = cudaGraphLaunch(ex, stream);
+            else enqueue_step_launches(stream, pl, d);
+            if (e != cudaSuccess) return poison(e, "step");
+            for (firex_sim* s : members) s->advance_mirror();
+            if (!profiling) {
+                pendingLaunches[FIREX_PASS_OTHER] += 2;
+                pendingLaunches[FIREX_PASS_SIMULATE] += 1;
+                pendingLaunches[FIREX_PASS_DIVERGENCE] += 2;
+                pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
+                pendingLaunches[FIREX_PASS_PROJECT] += 2;
+            }
+        }
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return poison(e, "step launch");
+        return FIREX_OK;
+    }
+
+    int poison(cudaError_t e, const char* what) {
+        for (firex_sim* s : members) s->cuda_fail(e, what);
+        return fail(FIREX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+
+    void drop_graphs() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+
+    void destroy() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (cudaEvent_t e : evPool) cudaEventDestroy(e);
         evPool.clear();
-        evMarks.clear();
-        for (void* p : allocations) cudaFree(p);
-        allocations.clear();
+        if (d) cudaFree(d);
+        d = nullptr;
+        delete h;
+        h = nullptr;
         if (stream) cudaStreamDestroy(stream);
         stream = nullptr;
     }
 
-    // Bytes the resource set needs (what create allocates), for admission.
-    static size_t planned_bytes(long long N, int mode) {
-        size_t b = (size_t)N * (16 * 4 + 4 * 2 /*div, reaction*/ + 4 /*liquid*/ + 4 /*tmp*/);
-        if (mode == FIREX_PRESSURE_WARM_F32) b += (size_t)N * 16;  // 2 pressure + 2 correction
-        else b += (size_t)N * 8;                                    // 2 pressure (shared in branch C)
-        return b + 64 * 1024;
-    }
-
-    // writeUniforms (FireXEngine.ts:2043-2113) plus the emitter extension.
-    void build_params(FxParams& p, double dt) const {
-        std::memset(&p, 0, sizeof(p));
-        auto P = [&](const char* n) { return named[param_slot(n)]; };
-        const double cells = (double)X * (double)Y * (double)Z;
-        const double u[FIREX_UNIFORM_FLOATS] = {
-            (double)X, (double)Y, (double)Z, cells,
-            (double)dt, simTime, (double)frame, (double)dt,
-            P("fuelRate"), P("oxygenRate"), P("heatEfficiency"), P("vorticity"),
-            P("waterFlow"), (P("sprayAngle") * M_PI) / 180, P("waterEnabled") != 0 ? 1.0 : 0.0, 300,
-            P("cameraYaw"), P("cameraPitch"), P("cameraDistance"), 1,  // canvas aspect (presentation only)
-            1, 1, 0, 0,                                                // canvas size, rays, particles
-            P("viewMode"), P("aimHeight"), P("nozzleType"), P("exposure"),
-            P("burnerSize"), P("burnerDepth"), P("sourceThickness"), P("firePower"),
-            P("domainWidth"), P("domainHeight"), P("domainDepth"), 0,
-            P("sourceLift"), P("buoyancyScale"), P("flamePersistence"), P("viewZoom"),
-            P("airEntrainment"), P("frontDefinition"), opt.cinematic ? 1.0 : 0.0, P("opticalDetailTarget")};
-        for (int i = 0; i < FIREX_UNIFORM_FLOATS; ++i) p.u[i] = (float)u[i];
-        p.emitter_mode = opt.emitter_mode;
-        p.num_spheres = opt.emitter_mode == FIREX_EMITTER_SPHERES ? opt.num_spheres : 0;
-        for (int s = 0; s < FIREX_MAX_SPHERES; ++s) p.spheres[s] = opt.spheres[s];
-        p.jitter = jitter(frame);
-    }
-
-    // Seeded per-step emission factor in [1-a, 1+a] (extension): splitmix64 of the frame
-    // index, 24 random bits.
-    float jitter(int64_t f) const {
-        auto mix = [](uint64_t z) {
-            z += 0x9E3779B97F4A7C15ull;
-            z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-            z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-            return z ^ (z >> 31);
-        };
-        uint64_t h = mix(mix(opt.seed ^ 0xBB67AE8584CAA73Bull) + (uint64_t)f);
-        float u = (float)(h >> 40) * (1.0f / 16777216.0f);
-        return 1.0f + opt.emission_jitter * (2.0f * u - 1.0f);
-    }
-
-    int reset() {
-        simTime = 0;
-        frame = 0;
-        speciesIndex = 0;
-        pressureIndex = 0;
-        lastCorrection = 0;
-        lastCorrectionShared = mode == FIREX_PRESSURE_COLD_F32;
-        // clearBuffer on every field, then initializeFields (FireXEngine.ts:1948-1969)
-        const size_t v4 = (size_t)N * 16, s4 = (size_t)N * 4;
-        cudaMemsetAsync(flow[0], 0, v4, stream);
-        cudaMemsetAsync(flow[1], 0, v4, stream);
-        cudaMemsetAsync(species[0], 0, v4, stream);
-        cudaMemsetAsync(species[1], 0, v4, stream);
-        for (int i = 0; i < 2; ++i) {
-            cudaMemsetAsync(pressure[i], 0, s4, stream);
-            if (correction[i] && correction[i] != pressure[i]) cudaMemsetAsync(correction[i], 0, s4, stream);
+    static firex_batch* make(int device, bool solo, std::string* err) {
+        firex_batch* b = new (std::nothrow) firex_batch();
+        if (!b) return nullptr;
+        b->device = device;
+        b->isSolo = solo;
+        b->h = new (std::nothrow) FxBatchDev();
+        cudaError_t e = b->h ? cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) : cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) e = cudaMalloc(&b->d, sizeof(FxBatchDev));
+        if (e != cudaSuccess) {
+            if (err) *err = std::string("batch: ") + cudaGetErrorString(e);
+            cudaGetLastError();
+            b->destroy();
+            delete b;
+            return nullptr;
         }
-        cudaMemsetAsync(div, 0, s4, stream);
-        cudaMemsetAsync(reaction, 0, s4, stream);
-        cudaMemsetAsync(liquid, 0, s4, stream);
-        const float oxygen = (float)named[param_slot("oxygenRate")];
-        fx_launch_init(stream, grid(), flow[0], species[0], opt.seed, opt.velocity_noise, 300.0f, oxygen);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, "reset");
-        return FIREX_OK;
-    }
-
-    // One encodeSimulationStep (FireXEngine.ts:2115-2276) with copyFlow replaced by a
-    // swap of the flow[0] / flow[1] roles.
-    void enqueue_step(double dt) {
-        FxParams hp;
-        build_params(hp, dt);
-        begin_marks();
-        fx_launch_upload_params(stream, hp, d_params);
-        mark(FIREX_PASS_OTHER, 1);
-        const FxGrid g = grid();
-        const int s = speciesIndex;
-        fx_launch_simulate_f32(stream, d_params, g, flow[0], species[s], liquid, flow[1], species[1 - s], reaction);
-        mark(FIREX_PASS_SIMULATE, 1);
-        speciesIndex = 1 - s;
-        fx_launch_divergence_f32(stream, d_params, g, flow[1], div);
-        mark(FIREX_PASS_DIVERGENCE, 1);
-        const int P = opt.pressure_iterations, R = opt.correction_iterations;
-        const size_t s4 = (size_t)N * 4;
-        if (mode == FIREX_PRESSURE_COLD_F32) {
-            cudaMemsetAsync(pressure[0], 0, s4, stream);
-            pressureIndex = 0;
-            mark(FIREX_PASS_OTHER, 0);
-        }
-        for (int i = 0; i < P; ++i) {
-            fx_launch_jacobi_f32(stream, d_params, g, pressure[pressureIndex], div, pressure[1 - pressureIndex]);
-            pressureIndex = 1 - pressureIndex;
-        }
-        mark(FIREX_PASS_JACOBI, P);
-        fx_launch_project_f32(stream, d_params, g, flow[1], pressure[pressureIndex], flow[0]);
-        mark(FIREX_PASS_PROJECT, 1);
-        fx_launch_divergence_f32(stream, d_params, g, flow[0], div);
-        mark(FIREX_PASS_DIVERGENCE, 1);
-        float** corr = (mode == FIREX_PRESSURE_COLD_F32) ? pressure : correction;
-        cudaMemsetAsync(corr[0], 0, s4, stream);
-        mark(FIREX_PASS_OTHER, 0);
-        int ci = 0;
-        for (int i = 0; i < R; ++i) {
-            fx_launch_jacobi_f32(stream, d_params, g, corr[ci], div, corr[1 - ci]);
-            ci = 1 - ci;
-        }
-        mark(FIREX_PASS_JACOBI, R);
-        fx_launch_project_f32(stream, d_params, g, flow[0], corr[ci], flow[1]);
-        mark(FIREX_PASS_PROJECT, 1);
-        std::swap(flow[0], flow[1]);
-        lastCorrection = ci;
-        lastCorrectionShared = mode == FIREX_PRESSURE_COLD_F32;
-        simTime += dt;
-        frame += 1;
+        b->rebuild_table();
+        return b;
     }
 };
+
+cudaStream_t firex_sim::stream() const { return batch ? batch->stream : solo->stream; }
+
+int firex_sim::reset() {
+    // FireXEngine.reset (FireXEngine.ts:843-852): counters to zero, every field cleared
+    // (clearBuffer, :1948-1961), then initializeFields (:1962-1969).
+    cudaStream_t st = stream();
+    h.simTime = 0;
+    h.frame = 0;
+    h.fi = h.si = h.pi = 0;
+    refresh_params();
+    flush(st);
+    const size_t v4 = (size_t)N * 16;
+    for (int i = 0; i < 2; ++i) {
+        cudaMemsetAsync(h.flow[i], 0, v4, st);
+        cudaMemsetAsync(h.species[i], 0, (size_t)N * species_bytes(), st);
+        cudaMemsetAsync(h.p[i], 0, (size_t)N * pressure_bytes(), st);
+        if (h.corr[i] != h.p[i]) cudaMemsetAsync(h.corr[i], 0, (size_t)N * pressure_bytes(), st);
+    }
+    cudaMemsetAsync(h.div, 0, (size_t)N * 4, st);
+    cudaMemsetAsync(h.reaction, 0, (size_t)N * 4, st);
+    cudaMemsetAsync(h.liquid, 0, (size_t)N * 4, st);
+    fx_launch_init(st, storage, d, 300.0f, (float)named[param_slot("oxygenRate")], opt.velocity_noise);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "reset");
+    return FIREX_OK;
+}
+
+void firex_sim::release() {
+    if (batch) cudaStreamSynchronize(batch->stream);  // no batch work may still use the buffers
+    if (batch && batch != solo) {
+        auto& m = batch->members;
+        m.erase(std::remove(m.begin(), m.end(), this), m.end());
+        batch->rebuild_table();
+        batch->drop_graphs();
+        batch = nullptr;
+    }
+    if (solo) {
+        solo->destroy();
+        delete solo;
+        solo = nullptr;
+    }
+    if (own) cudaStreamSynchronize(own);
+    for (void* p : allocations) cudaFree(p);
+    allocations.clear();
+    if (own) cudaStreamDestroy(own);
+    own = nullptr;
+}
+
+// ---- host-side field conversion for the mixed storage -----------------------------------------
+static inline float half_bits_to_float(uint16_t hb) {
+    __half hv;
+    std::memcpy(&hv, &hb, 2);
+    return __half2float(hv);
+}
+static inline uint16_t float_to_half_bits(float f) {
+    __half hv = __float2half_rn(f);
+    uint16_t hb;
+    std::memcpy(&hb, &hv, 2);
+    return hb;
+}
 
 // ---- C ABI ---------------------------------------------------------------------------------
 extern "C" {
@@ -366,6 +714,15 @@ uint64_t firex_reference_memory_estimate(const int32_t dims[3], int64_t particle
     return cells * per + (uint64_t)std::max<int64_t>(particle_count, 0) * 80 + 64ull * 64 * 64 * 4;
 }
 
+uint64_t firex_planned_device_bytes(const int32_t dims[3], const firex_options* opt) {
+    if (!dims || !opt) return 0;
+    const long long N = (long long)std::max(dims[0], 0) * std::max(dims[1], 0) * std::max(dims[2], 0);
+    int mode = opt->pressure_mode;
+    if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
+    const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
+    return firex_sim::planned_bytes(N, storage, mode);
+}
+
 int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** out) {
     if (!out) return FIREX_ERR_BAD_ARG;
     *out = nullptr;
@@ -374,13 +731,15 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         return FIREX_ERR_BAD_ARG;
     }
     for (int i = 0; i < 3; ++i)
-        if (dims[i] <= 0 || dims[i] % 4 != 0 || dims[i] > 2048) {
+        if (dims[i] < 4 || dims[i] % 4 != 0 || dims[i] > 2048) {
             g_create_error = "grid axes must be positive multiples of 4 and at most 2048";
             return FIREX_ERR_BAD_ARG;
         }
-    if (opt->pressure_iterations < 0 || opt->correction_iterations < 0 || opt->num_spheres < 0 ||
-        opt->num_spheres > FIREX_MAX_SPHERES || (opt->emitter_mode != FIREX_EMITTER_BURNER && opt->emitter_mode != FIREX_EMITTER_SPHERES) ||
+    if (opt->pressure_iterations < 0 || opt->correction_iterations < 0 || opt->pressure_iterations > 100000 ||
+        opt->correction_iterations > 100000 || opt->num_spheres < 0 || opt->num_spheres > FIREX_MAX_SPHERES ||
+        (opt->emitter_mode != FIREX_EMITTER_BURNER && opt->emitter_mode != FIREX_EMITTER_SPHERES) ||
         opt->pressure_mode < FIREX_PRESSURE_AUTO || opt->pressure_mode > FIREX_PRESSURE_COLD_F32 ||
+        (opt->precision != FIREX_PRECISION_F32 && opt->precision != FIREX_PRECISION_MIXED) ||
         !(opt->velocity_noise >= 0) || !(opt->emission_jitter >= 0)) {
         g_create_error = "invalid options";
         return FIREX_ERR_BAD_ARG;
@@ -392,11 +751,12 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
     }
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
-    if (mode == FIREX_PRESSURE_F16 || opt->precision != FIREX_PRECISION_F32) {
-        g_create_error = "f16 pressure storage and mixed precision are not available in this build";
+    const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
+    if (storage == FX_STORAGE_MIXED && mode == FIREX_PRESSURE_COLD_F32) {
+        g_create_error = "mixed precision stores pressure in FP16; the cold f32 branch does not apply";
         return FIREX_ERR_UNSUPPORTED;
     }
-    const size_t need = firex_sim::planned_bytes(N, mode);
+    const size_t need = firex_sim::planned_bytes(N, storage, mode);
     if (opt->memory_budget_bytes && need > opt->memory_budget_bytes) {
         g_create_error = "grid needs " + std::to_string(need) + " device bytes, above the " +
                          std::to_string(opt->memory_budget_bytes) + "-byte budget";
@@ -410,9 +770,16 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
     s->N = N;
     s->opt = *opt;
     s->mode = mode;
+    s->storage = storage;
+    s->half = storage == FX_STORAGE_MIXED || mode == FIREX_PRESSURE_F16;
     for (int i = 0; i < kNumParams; ++i) s->named[i] = kParams[i].def;
+    if (opt->jacobi_block > 1) {
+        s->jacobiKernel = FIREX_JACOBI_FUSED;
+        s->jacobiK = opt->jacobi_block;
+    }
+    s->jacobiZc = std::max(0, opt->jacobi_zchunk);
     cudaError_t e = cudaGetDevice(&s->device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         g_create_error = std::string("CUDA unavailable: ") + cudaGetErrorString(e);
         cudaGetLastError();
@@ -426,25 +793,44 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         delete s;
         return FIREX_ERR_OOM;
     }
-    bool ok = true;
+    s->solo = firex_batch::make(s->device, true, &g_create_error);
+    bool ok = s->solo != nullptr;
+    FxSimDev& h = s->h;
+    std::memset(&h, 0, sizeof(h));
+    h.X = s->X;
+    h.Y = s->Y;
+    h.Z = s->Z;
+    h.P = opt->pressure_iterations;
+    h.R = opt->correction_iterations;
+    h.mode = mode;
+    h.storage = storage;
+    h.active = 1;
+    h.seed = opt->seed;
+    h.jitterAmp = opt->emission_jitter;
+    h.dt = 1.0 / 60.0;
+    const size_t pb = s->pressure_bytes();
     for (int i = 0; i < 2 && ok; ++i) {
-        ok = (s->flow[i] = s->alloc<float4>(N)) && (s->species[i] = s->alloc<float4>(N)) &&
-             (s->pressure[i] = s->alloc<float>(N));
-        if (ok && mode == FIREX_PRESSURE_WARM_F32) ok = (s->correction[i] = s->alloc<float>(N)) != nullptr;
-        if (ok && mode == FIREX_PRESSURE_COLD_F32) s->correction[i] = s->pressure[i];
+        ok = (h.flow[i] = s->alloc((size_t)N * 16)) && (h.species[i] = s->alloc((size_t)N * s->species_bytes())) &&
+             (h.p[i] = s->alloc((size_t)N * pb));
+        if (ok) h.corr[i] = (mode == FIREX_PRESSURE_COLD_F32) ? h.p[i] : s->alloc((size_t)N * pb);
+        ok = ok && h.corr[i];
     }
-    ok = ok && (s->div = s->alloc<float>(N)) && (s->reaction = s->alloc<float>(N)) && (s->liquid = s->alloc<uint32_t>(N)) &&
-         (s->d_tmp = s->alloc<float>(N)) && (s->d_params = s->alloc<FxParams>(1)) &&
-         (s->d_partial = s->alloc<double>(2 * (size_t)fx_norm_partial_blocks(s->grid()))) && (s->d_norm = s->alloc<double>(2));
+    ok = ok && (h.div = (float*)s->alloc((size_t)N * 4)) && (h.reaction = (float*)s->alloc((size_t)N * 4)) &&
+         (h.liquid = (uint32_t*)s->alloc((size_t)N * 4)) && (s->d_tmp = s->alloc((size_t)N * 4)) &&
+         (s->d = (FxSimDev*)s->alloc(sizeof(FxSimDev))) &&
+         (s->d_partial = (double*)s->alloc(2 * sizeof(double) * (size_t)fx_norm_partial_blocks(N))) &&
+         (s->d_norm = (double*)s->alloc(2 * sizeof(double)));
     if (!ok) {
-        g_create_error = "device allocation failed (" + std::to_string(need) + " bytes requested)";
+        if (g_create_error.empty() || s->solo) g_create_error = "device allocation failed (" + std::to_string(need) + " bytes requested)";
         s->release();
         delete s;
         return FIREX_ERR_OOM;
     }
+    s->solo->members.push_back(s);
+    s->solo->rebuild_table();
     int rc = s->reset();
     if (rc == FIREX_OK) {
-        e = cudaStreamSynchronize(s->stream);
+        e = cudaStreamSynchronize(s->stream());
         if (e != cudaSuccess) rc = s->cuda_fail(e, "initialise");
     }
     if (rc != FIREX_OK) {
@@ -453,6 +839,7 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         delete s;
         return rc;
     }
+    g_create_error.clear();
     *out = s;
     return FIREX_OK;
 }
@@ -474,6 +861,7 @@ int firex_set_parameter(firex_sim* s, const char* name, int32_t kind, double val
     int i = param_slot(name);
     if (i < 0) return FIREX_OK;  // unknown names are ignored (FireXEngine.ts:1029-1030)
     s->named[i] = apply_rule(kParams[i], s->named[i], kind, value);
+    s->refresh_params();
     return FIREX_OK;
 }
 
@@ -495,70 +883,74 @@ int firex_reset(firex_sim* s) {
 int firex_step(firex_sim* s, int32_t nsteps, double dt) {
     if (!s) return FIREX_ERR_BAD_ARG;
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
+    if (s->batch) return s->fail(FIREX_ERR_STATE, "the simulation is a member of a batch; step the batch");
     if (nsteps < 0 || !std::isfinite(dt) || dt < 0) return s->fail(FIREX_ERR_BAD_ARG, "step count and dt must be finite and non-negative");
-    DeviceGuard dg(s->device);
-    for (int i = 0; i < nsteps; ++i) s->enqueue_step(dt);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return s->cuda_fail(e, "step launch");
-    return FIREX_OK;
+    int rc = s->solo->step(nsteps, dt);
+    if (rc != FIREX_OK && s->err.empty()) s->err = s->solo->err;
+    return rc;
 }
 
 int firex_sync(firex_sim* s) {
     if (!s) return FIREX_ERR_BAD_ARG;
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
     DeviceGuard dg(s->device);
-    cudaError_t e = cudaStreamSynchronize(s->stream);
+    cudaError_t e = cudaStreamSynchronize(s->stream());
     if (e != cudaSuccess) return s->cuda_fail(e, "sync");
     return FIREX_OK;
 }
 
-static int field_ptr(firex_sim* s, int32_t field, bool writing, void** ptr) {
+// Device buffer and element size backing a field in the current parity, for direct copies.
+static void* field_buffer(firex_sim* s, int32_t field) {
+    const FxSimDev& h = s->h;
     switch (field) {
-        case FIREX_FIELD_FLOW: *ptr = s->flow[0]; return FIREX_OK;
-        case FIREX_FIELD_SPECIES: *ptr = s->species[s->speciesIndex]; return FIREX_OK;
-        case FIREX_FIELD_PRESSURE: *ptr = s->pressure[s->pressureIndex]; return FIREX_OK;
-        case FIREX_FIELD_DIVERGENCE: *ptr = s->div; return FIREX_OK;
-        case FIREX_FIELD_REACTION: *ptr = s->reaction; return FIREX_OK;
-        case FIREX_FIELD_LIQUID: *ptr = s->liquid; return FIREX_OK;
-        case FIREX_FIELD_CORRECTION:
-            if (writing) return FIREX_ERR_BAD_ARG;
-            *ptr = s->lastCorrectionShared ? s->pressure[s->lastCorrection] : s->correction[s->lastCorrection];
-            return FIREX_OK;
-        case FIREX_FIELD_EMITTER_MASK:
-            if (writing) return FIREX_ERR_BAD_ARG;
-            {
-                FxParams hp;
-                s->build_params(hp, 0.0f);
-                fx_launch_upload_params(s->stream, hp, s->d_params);
-                fx_launch_emitter_mask(s->stream, s->d_params, s->grid(), reinterpret_cast<uint8_t*>(s->d_tmp));
-            }
-            *ptr = s->d_tmp;
-            return FIREX_OK;
-        case FIREX_FIELD_FINAL_DIVERGENCE:
-            if (writing) return FIREX_ERR_BAD_ARG;
-            {
-                FxParams hp;
-                s->build_params(hp, 0.0f);
-                fx_launch_upload_params(s->stream, hp, s->d_params);
-                fx_launch_divergence_f32(s->stream, s->d_params, s->grid(), s->flow[0], s->d_tmp);
-            }
-            *ptr = s->d_tmp;
-            return FIREX_OK;
+        case FIREX_FIELD_FLOW: return h.flow[h.fi];
+        case FIREX_FIELD_SPECIES: return h.species[h.si];
+        case FIREX_FIELD_PRESSURE: return h.p[h.pi];
+        case FIREX_FIELD_DIVERGENCE: return h.div;
+        case FIREX_FIELD_REACTION: return h.reaction;
+        case FIREX_FIELD_LIQUID: return h.liquid;
+        case FIREX_FIELD_CORRECTION: return h.corr[h.R & 1];
     }
-    return FIREX_ERR_BAD_ARG;
+    return nullptr;
 }
 
 int firex_read_field(firex_sim* s, int32_t field, void* host, size_t bytes) {
     if (!s || !host) return FIREX_ERR_BAD_ARG;
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
-    size_t es = firex_field_element_size(field);
+    const size_t es = firex_field_element_size(field);
     if (!es) return s->fail(FIREX_ERR_BAD_ARG, "unknown field id");
     if (bytes != es * (size_t)s->N) return s->fail(FIREX_ERR_BAD_ARG, "byte count does not match the field size");
     DeviceGuard dg(s->device);
-    void* src = nullptr;
-    if (field_ptr(s, field, false, &src) != FIREX_OK) return s->fail(FIREX_ERR_BAD_ARG, "field is not readable");
-    cudaError_t e = cudaMemcpyAsync(host, src, bytes, cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaStream_t st = s->stream();
+    cudaError_t e = cudaSuccess;
+    const size_t N = (size_t)s->N;
+    if (field == FIREX_FIELD_EMITTER_MASK || field == FIREX_FIELD_FINAL_DIVERGENCE) {
+        s->flush(st);
+        if (field == FIREX_FIELD_EMITTER_MASK) fx_launch_emitter_mask(st, s->d, (uint8_t*)s->d_tmp);
+        else fx_launch_final_divergence(st, s->d, (float*)s->d_tmp);
+        e = cudaMemcpyAsync(host, s->d_tmp, bytes, cudaMemcpyDeviceToHost, st);
+    } else if ((field == FIREX_FIELD_CORRECTION && s->h.R == 0) ||
+               (field == FIREX_FIELD_PRESSURE && s->mode == FIREX_PRESSURE_COLD_F32 &&
+                (s->h.R == 0 || (s->h.R == 1 && s->h.pi == 0)))) {
+        // Buffers the reference clears before the residual solve and no sweep rewrote
+        // (FireXEngine.ts:2229-2230, :2258-2259): they read as zero.
+        std::memset(host, 0, bytes);
+    } else if (field == FIREX_FIELD_SPECIES && s->storage == FX_STORAGE_MIXED) {
+        std::vector<uint16_t> raw(N * 4);
+        e = cudaMemcpyAsync(raw.data(), field_buffer(s, field), N * 8, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        float* o = (float*)host;
+        for (size_t i = 0; i < N * 4; ++i) o[i] = half_bits_to_float(raw[i]);
+    } else if ((field == FIREX_FIELD_PRESSURE || field == FIREX_FIELD_CORRECTION) && s->half) {
+        std::vector<uint16_t> raw(N);
+        e = cudaMemcpyAsync(raw.data(), field_buffer(s, field), N * 2, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        float* o = (float*)host;
+        for (size_t i = 0; i < N; ++i) o[i] = half_bits_to_float(raw[i]);
+    } else {
+        e = cudaMemcpyAsync(host, field_buffer(s, field), bytes, cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return s->cuda_fail(e, "read_field");
     return FIREX_OK;
 }
@@ -566,14 +958,31 @@ int firex_read_field(firex_sim* s, int32_t field, void* host, size_t bytes) {
 int firex_write_field(firex_sim* s, int32_t field, const void* host, size_t bytes) {
     if (!s || !host) return FIREX_ERR_BAD_ARG;
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
-    size_t es = firex_field_element_size(field);
+    const size_t es = firex_field_element_size(field);
     if (!es) return s->fail(FIREX_ERR_BAD_ARG, "unknown field id");
     if (bytes != es * (size_t)s->N) return s->fail(FIREX_ERR_BAD_ARG, "byte count does not match the field size");
+    if (field == FIREX_FIELD_EMITTER_MASK || field == FIREX_FIELD_FINAL_DIVERGENCE || field == FIREX_FIELD_CORRECTION)
+        return s->fail(FIREX_ERR_BAD_ARG, "field is read only");
     DeviceGuard dg(s->device);
-    void* dst = nullptr;
-    if (field_ptr(s, field, true, &dst) != FIREX_OK) return s->fail(FIREX_ERR_BAD_ARG, "field is not writable");
-    cudaError_t e = cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaStream_t st = s->stream();
+    const size_t N = (size_t)s->N;
+    cudaError_t e;
+    if (field == FIREX_FIELD_SPECIES && s->storage == FX_STORAGE_MIXED) {
+        std::vector<uint16_t> raw(N * 4);
+        const float* in = (const float*)host;
+        for (size_t i = 0; i < N * 4; ++i) raw[i] = float_to_half_bits(in[i]);
+        e = cudaMemcpyAsync(field_buffer(s, field), raw.data(), N * 8, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    } else if (field == FIREX_FIELD_PRESSURE && s->half) {
+        std::vector<uint16_t> raw(N);
+        const float* in = (const float*)host;
+        for (size_t i = 0; i < N; ++i) raw[i] = float_to_half_bits(in[i]);
+        e = cudaMemcpyAsync(field_buffer(s, field), raw.data(), N * 2, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    } else {
+        e = cudaMemcpyAsync(field_buffer(s, field), host, bytes, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
     if (e != cudaSuccess) return s->cuda_fail(e, "write_field");
     return FIREX_OK;
 }
@@ -582,26 +991,25 @@ int firex_divergence_norm(firex_sim* s, double out[3]) {
     if (!s || !out) return FIREX_ERR_BAD_ARG;
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
     DeviceGuard dg(s->device);
-    FxParams hp;
-    s->build_params(hp, 0.0f);
-    fx_launch_upload_params(s->stream, hp, s->d_params);
-    fx_launch_divergence_norm(s->stream, s->d_params, s->grid(), s->flow[0], s->d_partial, s->d_norm);
-    double h[2] = {0, 0};
-    cudaError_t e = cudaMemcpyAsync(h, s->d_norm, sizeof(h), cudaMemcpyDeviceToHost, s->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaStream_t st = s->stream();
+    s->flush(st);
+    fx_launch_divergence_norm(st, s->d, s->N, s->d_partial, s->d_norm);
+    double hbuf[2] = {0, 0};
+    cudaError_t e = cudaMemcpyAsync(hbuf, s->d_norm, sizeof(hbuf), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return s->cuda_fail(e, "divergence_norm");
-    out[0] = h[0];
-    out[1] = h[1];
+    out[0] = hbuf[0];
+    out[1] = hbuf[1];
     out[2] = (double)(s->X - 2) * (double)(s->Y - 2) * (double)(s->Z - 2);
     return FIREX_OK;
 }
 
 int firex_get_state(const firex_sim* s, firex_state* st) {
     if (!s || !st) return FIREX_ERR_BAD_ARG;
-    st->simulation_time = s->simTime;
-    st->frame_index = s->frame;
-    st->species_index = s->speciesIndex;
-    st->pressure_index = s->pressureIndex;
+    st->simulation_time = s->h.simTime;
+    st->frame_index = s->h.frame;
+    st->species_index = s->h.si;
+    st->pressure_index = s->h.pi;
     return FIREX_OK;
 }
 
@@ -609,10 +1017,14 @@ int firex_set_state(firex_sim* s, const firex_state* st) {
     if (!s || !st) return FIREX_ERR_BAD_ARG;
     if ((st->species_index & ~1) || (st->pressure_index & ~1) || !std::isfinite(st->simulation_time))
         return s->fail(FIREX_ERR_BAD_ARG, "invalid state");
-    s->simTime = st->simulation_time;
-    s->frame = st->frame_index;
-    s->speciesIndex = st->species_index;
-    s->pressureIndex = st->pressure_index;
+    DeviceGuard dg(s->device);
+    cudaStreamSynchronize(s->stream());
+    s->h.simTime = st->simulation_time;
+    s->h.frame = st->frame_index;
+    s->h.si = st->species_index;
+    s->h.pi = st->pressure_index;
+    s->refresh_params();
+    s->flush(s->stream());
     return FIREX_OK;
 }
 
@@ -644,29 +1056,163 @@ int firex_device_bytes(const firex_sim* s, uint64_t* bytes) {
     return FIREX_OK;
 }
 
-void* firex_stream(const firex_sim* s) { return s ? (void*)s->stream : nullptr; }
+void* firex_stream(const firex_sim* s) { return s ? (void*)s->stream() : nullptr; }
 
 int firex_set_profiling(firex_sim* s, int32_t on) {
     if (!s) return FIREX_ERR_BAD_ARG;
+    firex_batch* b = s->batch ? s->batch : s->solo;
     DeviceGuard dg(s->device);
-    if (!on && s->profiling) s->collect_marks();
-    s->profiling = on != 0;
+    if (!on && b->profiling) b->collect_marks();
+    b->profiling = on != 0;
     return FIREX_OK;
 }
 
 int firex_pass_times(firex_sim* s, double* ms, int64_t* launches) {
     if (!s) return FIREX_ERR_BAD_ARG;
-    if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
+    firex_batch* b = s->batch ? s->batch : s->solo;
     DeviceGuard dg(s->device);
-    int rc = s->collect_marks();
-    if (rc != FIREX_OK) return rc;
+    int rc = b->collect_marks();
+    if (rc != FIREX_OK) return s->fail(rc, b->err);
     for (int p = 0; p < FIREX_PASS_COUNT; ++p) {
-        if (ms) ms[p] = s->passMs[p];
-        if (launches) launches[p] = s->passLaunches[p];
-        s->passMs[p] = 0;
-        s->passLaunches[p] = 0;
+        if (ms) ms[p] = b->passMs[p];
+        if (launches) launches[p] = b->passLaunches[p];
+        b->passMs[p] = 0;
+        b->passLaunches[p] = 0;
     }
     return FIREX_OK;
 }
+
+int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
+    if (!s || !out) return FIREX_ERR_BAD_ARG;
+    std::memset(out, 0, sizeof(*out));
+    const firex_batch* b = s->batch ? s->batch : s->solo;
+    const StepPlan& p = b->last;
+    out->fast_division = s->h.jcFastDiv;
+    out->jacobi_block = p.k;
+    out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
+    out->graph = b->lastGraph ? 1 : 0;
+    out->launches_per_step = 7 + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+    return FIREX_OK;
+}
+
+static bool jacobi_args_ok(int32_t kernel, int32_t block, int32_t zchunk) {
+    if (kernel < FIREX_JACOBI_AUTO || kernel > FIREX_JACOBI_FUSED || zchunk < 0 || zchunk > 4096) return false;
+    return kernel != FIREX_JACOBI_FUSED || block == 2 || block == 3 || block == 4 || block == 6;
+}
+
+int firex_set_jacobi(firex_sim* s, int32_t kernel, int32_t block, int32_t zchunk) {
+    if (!s || !jacobi_args_ok(kernel, block, zchunk)) return FIREX_ERR_BAD_ARG;
+    s->jacobiKernel = kernel;
+    s->jacobiK = kernel == FIREX_JACOBI_FUSED ? block : 1;
+    s->jacobiZc = zchunk;
+    return FIREX_OK;
+}
+
+int firex_batch_set_jacobi(firex_batch* b, int32_t kernel, int32_t block, int32_t zchunk) {
+    if (!b || !jacobi_args_ok(kernel, block, zchunk)) return FIREX_ERR_BAD_ARG;
+    b->jacobiKernel = kernel;
+    b->jacobiK = kernel == FIREX_JACOBI_FUSED ? block : 1;
+    b->jacobiZc = zchunk;
+    return FIREX_OK;
+}
+
+int firex_set_graphs(firex_sim* s, int32_t on) {
+    if (!s) return FIREX_ERR_BAD_ARG;
+    s->solo->useGraphs = on != 0;
+    return FIREX_OK;
+}
+
+// ---- batches -------------------------------------------------------------------------------
+int firex_batch_create(firex_batch** out) {
+    if (!out) return FIREX_ERR_BAD_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        g_create_error = "CUDA unavailable";
+        return FIREX_ERR_CUDA;
+    }
+    *out = firex_batch::make(dev, false, &g_create_error);
+    return *out ? FIREX_OK : FIREX_ERR_OOM;
+}
+
+int firex_batch_destroy(firex_batch* b) {
+    if (!b) return FIREX_ERR_BAD_ARG;
+    DeviceGuard dg(b->device);
+    cudaStreamSynchronize(b->stream);
+    for (firex_sim* s : b->members) {
+        cudaEvent_t ev;
+        cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        cudaEventRecord(ev, b->stream);
+        cudaStreamWaitEvent(s->solo->stream, ev, 0);
+        cudaEventDestroy(ev);
+        s->batch = nullptr;
+    }
+    b->members.clear();
+    b->destroy();
+    delete b;
+    return FIREX_OK;
+}
+
+const char* firex_batch_last_error(const firex_batch* b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+int firex_batch_add(firex_batch* b, firex_sim* s) {
+    if (!b || !s) return FIREX_ERR_BAD_ARG;
+    if (s->batch) return b->fail(FIREX_ERR_STATE, "the simulation already belongs to a batch");
+    if (s->poisoned) return b->fail(FIREX_ERR_STATE, "the simulation is poisoned");
+    if (s->device != b->device) return b->fail(FIREX_ERR_BAD_ARG, "the simulation lives on another device");
+    if ((int)b->members.size() >= FX_MAX_BATCH) return b->fail(FIREX_ERR_BUDGET, "batch is full");
+    if (!b->members.empty() && (b->members[0]->storage != s->storage || b->members[0]->half != s->half))
+        return b->fail(FIREX_ERR_UNSUPPORTED, "batch members must share storage precision and pressure storage");
+    DeviceGuard dg(b->device);
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventRecord(ev, s->solo->stream);
+    cudaStreamWaitEvent(b->stream, ev, 0);  // the batch runs after the sim's queued work
+    cudaEventDestroy(ev);
+    s->batch = b;
+    s->dirty = true;
+    b->members.push_back(s);
+    b->rebuild_table();
+    return FIREX_OK;
+}
+
+int firex_batch_remove(firex_batch* b, firex_sim* s) {
+    if (!b || !s) return FIREX_ERR_BAD_ARG;
+    if (s->batch != b) return b->fail(FIREX_ERR_BAD_ARG, "the simulation is not a member of this batch");
+    DeviceGuard dg(b->device);
+    cudaEvent_t ev;
+    cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    cudaEventRecord(ev, b->stream);
+    cudaStreamWaitEvent(s->solo->stream, ev, 0);  // later sim work runs after the batch's
+    cudaEventDestroy(ev);
+    auto& m = b->members;
+    m.erase(std::remove(m.begin(), m.end(), s), m.end());
+    s->batch = nullptr;
+    s->dirty = true;
+    b->rebuild_table();
+    return FIREX_OK;
+}
+
+int firex_batch_size(const firex_batch* b, int32_t* n) {
+    if (!b || !n) return FIREX_ERR_BAD_ARG;
+    *n = (int32_t)b->members.size();
+    return FIREX_OK;
+}
+
+int firex_batch_step(firex_batch* b, int32_t nsteps, double dt) {
+    if (!b) return FIREX_ERR_BAD_ARG;
+    if (nsteps < 0 || !std::isfinite(dt) || dt < 0) return b->fail(FIREX_ERR_BAD_ARG, "step count and dt must be finite and non-negative");
+    return b->step(nsteps, dt);
+}
+
+int firex_batch_sync(firex_batch* b) {
+    if (!b) return FIREX_ERR_BAD_ARG;
+    DeviceGuard dg(b->device);
+    cudaError_t e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return b->poison(e, "batch sync");
+    return FIREX_OK;
+}
+
+void* firex_batch_stream(const firex_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"

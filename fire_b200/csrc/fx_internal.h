@@ -8,17 +8,29 @@
 
 #include "fx_device.cuh"
 
-// ---- plain FP32 passes (fx_kernels_f32.cu) -------------------------------------------------
-void fx_launch_simulate_f32(cudaStream_t s, const FxParams* prm, FxGrid g, const float4* flowIn, const float4* speciesIn,
-                            const uint32_t* liquid, float4* flowOut, float4* speciesOut, float* reaction);
-void fx_launch_divergence_f32(cudaStream_t s, const FxParams* prm, FxGrid g, const float4* flow, float* div);
-void fx_launch_jacobi_f32(cudaStream_t s, const FxParams* prm, FxGrid g, const float* pin, const float* div, float* pout);
-void fx_launch_project_f32(cudaStream_t s, const FxParams* prm, FxGrid g, const float4* flowIn, const float* p,
-                           float4* flowOut);
-void fx_launch_init(cudaStream_t s, FxGrid g, float4* flow, float4* species, uint64_t seed, float noise, float tAmbient,
-                    float oxygen);
-void fx_launch_emitter_mask(cudaStream_t s, const FxParams* prm, FxGrid g, uint8_t* mask);
-int fx_norm_partial_blocks(FxGrid g);
-void fx_launch_divergence_norm(cudaStream_t s, const FxParams* prm, FxGrid g, const float4* flow, double* partial,
-                               double* out);
-void fx_launch_upload_params(cudaStream_t s, const FxParams& host, FxParams* dev);
+// Batched step passes (fx_kernels.cu). `bricks` is the batch's brick total for the
+// pass's shape; grids are persistent (full residency) capped at that total.
+void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B);
+void fx_launch_step_end(cudaStream_t s, FxBatchDev* B);
+void fx_launch_simulate(cudaStream_t s, int storage, const FxBatchDev* B, int bricks);
+void fx_launch_divergence(cudaStream_t s, const FxBatchDev* B, int bricks, int phase);
+void fx_launch_jacobi(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase, int launch, int sweep);
+// One sweep by z-marching tiles of zc planes (fx_jacobi_zm.cuh).
+void fx_launch_jacobi_zm(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase, int launch, int sweep,
+                         int zc);
+// K fused sweeps per launch; pmode selects the pressure storage and rounding.
+enum { FX_TB_F32 = 0, FX_TB_F16_ROUND = 1, FX_TB_F16 = 2 };
+bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc);
+void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase);
+
+// Single-simulation utilities.
+void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbient, float oxygen, float noise);
+void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask);
+void fx_launch_final_divergence(cudaStream_t s, const FxSimDev* S, float* out);
+int fx_norm_partial_blocks(long long cells);
+void fx_launch_divergence_norm(cudaStream_t s, const FxSimDev* S, long long cells, double* partial, double* out);
+void fx_launch_upload_desc(cudaStream_t s, const FxSimDev& host, FxSimDev* dev);
+void fx_launch_upload_batch(cudaStream_t s, const FxBatchDev& host, FxBatchDev* dev);
+
+// Exhaustive check of fx_div_by_const against IEEE division for one denominator.
+void fx_launch_check_div(cudaStream_t s, float d, float rcp, unsigned long long* mismatches);

@@ -1,0 +1,628 @@
+// fx_kernels.cu — the Fire-X step passes for sm_100a, batched.
+//
+// Every step pass takes an FxBatchDev: a device-resident list of simulation descriptors
+// (possibly of different grid sizes) and per-shape brick prefix sums. A pass is one
+// persistent launch whose CTAs stride over the flat brick list of the whole batch, so a
+// single simulation and a batch of uneven ones run the same code, and the launch
+// sequence of a step never depends on host-side values (graph-replayable).
+//
+// Compiled with --fmad=false: each reference expression is the same sequence of IEEE
+// operations as in the WGSL source (shaders.ts, pressureShaders.ts).
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+
+#include "fx_internal.h"
+#include "fx_jacobi_tb.cuh"
+#include "fx_jacobi_zm.cuh"
+#include "fx_step_math.cuh"
+#include "fx_storage.cuh"
+
+namespace {
+
+// ---- step prologue / epilogue ------------------------------------------------------------
+// Time fields of the uniform block for the step about to run (writeUniforms,
+// FireXEngine.ts:2049) and the per-step emission jitter (extension): splitmix64 of the
+// frame index, 24 random bits, same operations as the host.
+__global__ void fxk_step_begin(FxBatchDev* __restrict__ B) {
+    for (int s = threadIdx.x; s < B->nsims; s += blockDim.x) {
+        FxSimDev* S = B->sims[s];
+        if (!S->active) continue;
+        S->prm.u[U_DT] = (float)S->dt;
+        S->prm.u[U_TIME] = (float)S->simTime;
+        S->prm.u[6] = (float)S->frame;
+        S->prm.u[7] = (float)S->dt;
+        uint64_t h = fx_splitmix64(fx_splitmix64(S->seed ^ 0xBB67AE8584CAA73Bull) + (uint64_t)S->frame);
+        float u = __fmul_rn((float)(h >> 40), 1.0f / 16777216.0f);
+        S->prm.jitter = __fadd_rn(1.0f, __fmul_rn(S->jitterAmp, __fsub_rn(__fmul_rn(2.0f, u), 1.0f)));
+    }
+}
+
+// Counters after the step (renderOfflineFrameInternal, FireXEngine.ts:681-682) and the
+// ping-pong parities of encodeSimulationStep (:2172-2275); copyFlow is a parity flip.
+__global__ void fxk_step_end(FxBatchDev* __restrict__ B) {
+    for (int s = threadIdx.x; s < B->nsims; s += blockDim.x) {
+        FxSimDev* S = B->sims[s];
+        if (!S->active) continue;
+        S->simTime = S->simTime + S->dt;
+        S->frame += 1;
+        S->fi ^= 1;
+        S->si ^= 1;
+        S->pi = (S->mode == FIREX_PRESSURE_COLD_F32) ? (S->P & 1) : (S->pi ^ (S->P & 1));
+    }
+}
+
+// Per-brick iteration over a batch: calls body(S, brick-in-sim) for every brick of the
+// given shape. The owning simulation of consecutive bricks is cached.
+template <int SHAPE, class Body>
+FXD void fx_for_bricks(const FxBatchDev* __restrict__ B, Body body) {
+    const int total = B->total[SHAPE];
+    int lo = 0, hi = -1, s = 0;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        if (w < lo || w >= hi) {
+            s = fx_find_sim(B->start[SHAPE], B->nsims, w);
+            lo = __ldg(&B->start[SHAPE][s]);
+            hi = __ldg(&B->start[SHAPE][s + 1]);
+        }
+        const FxSimDev* S = B->sims[s];
+        if (!S->active) continue;
+        body(*S, w - lo);
+    }
+}
+
+// ---- simulate (shaders.ts:151-342) -------------------------------------------------------
+template <class St>
+struct Acc {
+    const void* flowIn;
+    const void* speciesIn;
+    const uint32_t* liq;
+    FXD float4 flow(long long i) const { return fx_ld_flow(flowIn, i); }
+    FXD float4 species(long long i) const { return St::ld_species(speciesIn, i); }
+    FXD uint32_t liquid(long long i) const { return __ldg(liq + i); }
+};
+
+template <class St>
+__global__ void __launch_bounds__(256) fxk_simulate(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_CELL>(B, [&](const FxSimDev& S, int b) {
+        const int nbx = (S.X + FX_CELL_BX - 1) / FX_CELL_BX, nby = (S.Y + FX_CELL_BY - 1) / FX_CELL_BY;
+        const int x = (b % nbx) * FX_CELL_BX + threadIdx.x % FX_CELL_BX;
+        const int y = ((b / nbx) % nby) * FX_CELL_BY + (threadIdx.x / FX_CELL_BX) % FX_CELL_BY;
+        const int z = (b / (nbx * nby)) * FX_CELL_BZ + threadIdx.x / (FX_CELL_BX * FX_CELL_BY);
+        if (x >= S.X || y >= S.Y || z >= S.Z) return;
+        const FxGrid g{S.X, S.Y, S.Z};
+        Acc<St> a{S.flow[S.fi], S.species[S.si], S.liquid};
+        FxCellOut o = fx_simulate_cell(S.prm, g, x, y, z, a);
+        const long long id = (long long)x + (long long)S.X * ((long long)y + (long long)S.Y * z);
+        fx_st_flow(S.flow[S.fi ^ 1], id, o.flow);
+        St::st_species(S.species[S.si ^ 1], id, o.species);
+        S.reaction[id] = o.reaction;
+    });
+}
+
+// ROW4 brick -> (x0, y, z) of this thread: 4 consecutive cells x0..x0+3. A simulation's
+// cells are split into X/4-cell groups in memory order (x fastest; rows are contiguous),
+// and brick b holds groups [256 b, 256 b + 256): consecutive threads touch consecutive
+// 16-byte segments, and no thread idles except at the end of the simulation.
+struct Row4 {
+    int x0, y, z;
+    bool ok;
+};
+FXD Row4 fx_row4(const FxSimDev& S, int b) {
+    const int gx = S.X >> 2;  // groups < 2^29: 32-bit arithmetic is exact
+    const int j = b * FX_ROW4_THREADS + (int)threadIdx.x;
+    const int t = j / gx;
+    Row4 r;
+    r.x0 = (j - t * gx) * 4;
+    r.z = t / S.Y;
+    r.y = t - r.z * S.Y;
+    r.ok = r.z < S.Z;
+    return r;
+}
+
+// ---- computeDivergence (shaders.ts:344-364) ---------------------------------------------
+// phase 0: the predicted flow after simulate; phase 1: the primary-projected flow (the
+// residual solve's right-hand side).
+__global__ void __launch_bounds__(256) fxk_divergence(const FxBatchDev* __restrict__ B, int phase) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+        const Row4 r = fx_row4(S, b);
+        if (!r.ok) return;
+        const void* flow = phase == 0 ? S.flow[S.fi ^ 1] : S.flow[S.fi];
+        const float3 m = fx_metric(S.prm.u);
+        const long long X = S.X, XY = (long long)S.X * S.Y;
+        const long long row = (long long)r.y * X + r.z * XY;
+        const long long rowB = (long long)(r.y > 0 ? r.y - 1 : 0) * X + r.z * XY;
+        const long long rowK = (long long)r.y * X + (long long)(r.z > 0 ? r.z - 1 : 0) * XY;
+        float left = fx_ld_flow(flow, row + (r.x0 > 0 ? r.x0 - 1 : 0)).x;
+        float d[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float4 c = fx_ld_flow(flow, row + r.x0 + i);
+            const float bottom = fx_ld_flow(flow, rowB + r.x0 + i).y;
+            const float back = fx_ld_flow(flow, rowK + r.x0 + i).z;
+            const float l = (i == 0 && r.x0 == 0) ? c.x : left;
+            d[i] = (c.x - l) * m.x + (c.y - bottom) * m.y + (c.z - back) * m.z;
+            left = c.x;
+        }
+        *reinterpret_cast<float4*>(S.div + row + r.x0) = make_float4(d[0], d[1], d[2], d[3]);
+    });
+}
+
+// ---- one Jacobi sweep (solvePressureGlobal, shaders.ts:375-403) --------------------------
+// phase 0: primary pressure, sweep index `sweep` of P (warm start from p[pi]; branch C
+// starts from zero); phase 1: residual pressure, sweep `sweep` of R, starting from zero.
+// A sweep whose input is known to be zero skips its loads: ((wx*(0+0) + ...) - div)/D is
+// exactly (0 - div)/D. Storage PT is float or half; the update is FP32.
+// Buffers of launch `launch` of a solve phase: launches alternate between the two
+// buffers of the phase starting from the warm-start parity (primary, branches A and B)
+// or from buffer 0 (residual, and the cold primary of branch C); the first launch of a
+// cleared solve has a zero input.
+struct FxSolveBufs {
+    const void* pin;
+    void* pout;
+    bool zeroIn;
+};
+FXD FxSolveBufs fx_solve_bufs(const FxSimDev& S, int phase, int launch) {
+    FxSolveBufs r;
+    if (phase == 0) {
+        const int base = (S.mode == FIREX_PRESSURE_COLD_F32) ? 0 : S.pi;
+        r.pin = S.p[(base + launch) & 1];
+        r.pout = S.p[(base + launch + 1) & 1];
+        r.zeroIn = S.mode == FIREX_PRESSURE_COLD_F32 && launch == 0;
+    } else {
+        r.pin = S.corr[launch & 1];
+        r.pout = S.corr[(launch + 1) & 1];
+        r.zeroIn = launch == 0;
+    }
+    return r;
+}
+
+template <typename PT>
+__global__ void __launch_bounds__(256) fxk_jacobi(const FxBatchDev* __restrict__ B, int phase, int launch, int sweep) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+        const int n = phase == 0 ? S.P : S.R;
+        if (sweep >= n) return;
+        const Row4 r = fx_row4(S, b);
+        if (!r.ok) return;
+        const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
+        const void* pin = bufs.pin;
+        void* pout = bufs.pout;
+        const bool zeroIn = bufs.zeroIn;
+        const long long X = S.X, XY = (long long)S.X * S.Y;
+        const long long row = (long long)r.y * X + r.z * XY;
+        if (r.y == S.Y - 1) {  // the open top is the ambient-pressure boundary
+            PStore<PT>::st4(pout, row + r.x0, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+            return;
+        }
+        const FxJacobiConst c{S.jc[0], S.jc[1], S.jc[2], S.jc[3]};
+        const float4 d = __ldg(reinterpret_cast<const float4*>(S.div + row + r.x0));
+        float4 o;
+        if (zeroIn) {
+            o = make_float4((0.0f - d.x) / c.denom, (0.0f - d.y) / c.denom, (0.0f - d.z) / c.denom, (0.0f - d.w) / c.denom);
+        } else {
+            const long long rowB = (long long)(r.y > 0 ? r.y - 1 : 0) * X + r.z * XY;
+            const long long rowT = (long long)(r.y + 1) * X + r.z * XY;
+            const long long rowK = (long long)r.y * X + (long long)(r.z > 0 ? r.z - 1 : 0) * XY;
+            const long long rowF = (long long)r.y * X + (long long)(r.z < S.Z - 1 ? r.z + 1 : r.z) * XY;
+            const float4 pc = PStore<PT>::ld4(pin, row + r.x0);
+            const float pl = r.x0 > 0 ? PStore<PT>::ld(pin, row + r.x0 - 1) : pc.x;
+            const float pr = r.x0 + 4 < S.X ? PStore<PT>::ld(pin, row + r.x0 + 4) : pc.w;
+            const float4 pb = PStore<PT>::ld4(pin, rowB + r.x0);
+            const float4 pt = PStore<PT>::ld4(pin, rowT + r.x0);
+            const float4 pk = PStore<PT>::ld4(pin, rowK + r.x0);
+            const float4 pf = PStore<PT>::ld4(pin, rowF + r.x0);
+            o.x = fx_jacobi_numerator(c, pl, pc.y, pb.x, pt.x, pk.x, pf.x, d.x);
+            o.y = fx_jacobi_numerator(c, pc.x, pc.z, pb.y, pt.y, pk.y, pf.y, d.y);
+            o.z = fx_jacobi_numerator(c, pc.y, pc.w, pb.z, pt.z, pk.z, pf.z, d.z);
+            o.w = fx_jacobi_numerator(c, pc.z, pr, pb.w, pt.w, pk.w, pf.w, d.w);
+            if (S.jcFastDiv) {
+                o = make_float4(fx_div_by_const(o.x, c.denom, S.jcRcp), fx_div_by_const(o.y, c.denom, S.jcRcp),
+                                fx_div_by_const(o.z, c.denom, S.jcRcp), fx_div_by_const(o.w, c.denom, S.jcRcp));
+            } else {
+                o = make_float4(o.x / c.denom, o.y / c.denom, o.z / c.denom, o.w / c.denom);
+            }
+        }
+        PStore<PT>::st4(pout, row + r.x0, o);
+    });
+}
+
+// ---- projectVelocity (shaders.ts:461-501, pressureShaders.ts:128-160) ------------------
+// phase 0: predicted flow F[1-fi] with the primary pressure -> F[fi];
+// phase 1: F[fi] with the residual pressure -> F[1-fi] (the step's result).
+// The solve's result sits in the buffer after its last launch; launch counts have the
+// parity of the sweep counts (the engine only fuses sweeps when they do), so the result
+// buffer is the reference's: p[(base + P) & 1] and corr[R & 1].
+template <typename PT>
+__global__ void __launch_bounds__(256) fxk_project(const FxBatchDev* __restrict__ B, int phase) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+        const Row4 r = fx_row4(S, b);
+        if (!r.ok) return;
+        const void* flowIn;
+        void* flowOut;
+        const void* p;
+        bool zeroP;
+        if (phase == 0) {
+            flowIn = S.flow[S.fi ^ 1];
+            flowOut = S.flow[S.fi];
+            const int base = (S.mode == FIREX_PRESSURE_COLD_F32) ? 0 : S.pi;
+            p = S.p[(base + S.P) & 1];
+            zeroP = S.mode == FIREX_PRESSURE_COLD_F32 && S.P == 0;
+        } else {
+            flowIn = S.flow[S.fi];
+            flowOut = S.flow[S.fi ^ 1];
+            p = S.corr[S.R & 1];
+            zeroP = S.R == 0;
+        }
+        const float3 m = fx_metric(S.prm.u);
+        const long long X = S.X, XY = (long long)S.X * S.Y;
+        const int ys = (r.y == S.Y - 1) ? r.y - 1 : r.y;  // top row: the projected row below
+        const long long row = (long long)r.y * X + r.z * XY;
+        const long long rowS = (long long)ys * X + r.z * XY;
+        float4 pc = make_float4(0, 0, 0, 0), pt = pc, pf = pc;
+        float pr = 0.0f;
+        if (!zeroP) {
+            pc = PStore<PT>::ld4(p, rowS + r.x0);
+            pr = r.x0 + 4 < S.X ? PStore<PT>::ld(p, rowS + r.x0 + 4) : pc.w;
+            pt = PStore<PT>::ld4(p, rowS + X + r.x0);  // ys + 1 <= Y - 1 always
+            pf = PStore<PT>::ld4(p, rowS + (r.z < S.Z - 1 ? XY : 0) + r.x0);
+        }
+        const float pcv[4] = {pc.x, pc.y, pc.z, pc.w};
+        const float pxv[4] = {pc.y, pc.z, pc.w, pr};
+        const float ptv[4] = {pt.x, pt.y, pt.z, pt.w};
+        const float pfv[4] = {pf.x, pf.y, pf.z, pf.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int x = r.x0 + i;
+            const float4 f = fx_ld_flow(flowIn, row + x);
+            const float4 src = (ys == r.y) ? f : fx_ld_flow(flowIn, rowS + x);
+            const float gx = (pxv[i] - pcv[i]) * m.x;
+            const float gy = (ptv[i] - pcv[i]) * m.y;
+            const float gz = (pfv[i] - pcv[i]) * m.z;
+            float4 o = make_float4(src.x - gx, src.y - gy, src.z - gz, f.w);
+            if (x == 0 || x == S.X - 1) o.x = 0.0f;
+            if (r.z == 0 || r.z == S.Z - 1) o.z = 0.0f;
+            if (r.y == 0) o.y = 0.0f;
+            if (r.y == S.Y - 1) o.y = fx_max(0.0f, o.y);
+            fx_st_flow(flowOut, row + x, o);
+        }
+    });
+}
+
+// ---- one Jacobi sweep by z-marching tiles (fx_jacobi_zm.cuh) ---------------------------------
+template <typename PT>
+__global__ void __launch_bounds__(FX_ZM_THREADS, 3) fxk_jacobi_zm(const FxBatchDev* __restrict__ B, int phase, int launch,
+                                                               int sweep, int zc) {
+    extern __shared__ __align__(16) unsigned char fx_zm_dyn[];
+    FxZmSmem<PT>& sm = *reinterpret_cast<FxZmSmem<PT>*>(fx_zm_dyn);
+    fx_for_bricks<FX_SHAPE_ZM>(B, [&](const FxSimDev& S, int b) {
+        const int n = phase == 0 ? S.P : S.R;
+        if (sweep >= n) return;
+        const int ntx = (S.X + FX_ZM_TX - 1) / FX_ZM_TX, nty = (S.Y + FX_ZM_TY - 1) / FX_ZM_TY;
+        const int tx = b % ntx, ty = (b / ntx) % nty, zci = b / (ntx * nty);
+        const int z0 = zci * zc, z1 = min(S.Z, z0 + zc);
+        const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
+        if (bufs.zeroIn)
+            fx_zm_tile<PT, true>(&S, reinterpret_cast<const PT*>(bufs.pin), reinterpret_cast<PT*>(bufs.pout),
+                                 tx * FX_ZM_TX, ty * FX_ZM_TY, z0, z1, sm);
+        else
+            fx_zm_tile<PT, false>(&S, reinterpret_cast<const PT*>(bufs.pin), reinterpret_cast<PT*>(bufs.pout),
+                                  tx * FX_ZM_TX, ty * FX_ZM_TY, z0, z1, sm);
+    });
+}
+
+// ---- K fused Jacobi sweeps per launch (fx_jacobi_tb.cuh) ------------------------------------
+template <int K, typename PT, bool ROUND>
+__global__ void __launch_bounds__(FX_TB_THREADS, 1) fxk_jacobi_tb(const FxBatchDev* __restrict__ B, int phase, int launch, int zc) {
+    extern __shared__ __align__(16) float fx_tb_dyn[];
+    auto sm = reinterpret_cast<float(*)[FX_TB_RY][FX_TB_RX]>(fx_tb_dyn);
+    auto dsm = reinterpret_cast<float(*)[FX_TB_RY][FX_TB_RX]>(fx_tb_dyn + K * FX_TB_RY * FX_TB_RX);
+    fx_for_bricks<FX_SHAPE_COL>(B, [&](const FxSimDev& S, int b) {
+        constexpr int TX = FxTbShape<K>::TX, TY = FxTbShape<K>::TY;
+        const int ntx = (S.X + TX - 1) / TX, nty = (S.Y + TY - 1) / TY;
+        const int tx = b % ntx, ty = (b / ntx) % nty, zci = b / (ntx * nty);
+        const int z0 = zci * zc, z1 = min(S.Z, z0 + zc);
+        const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
+        fx_tb_column<K, PT, ROUND>(S, bufs.pin, bufs.pout, bufs.zeroIn, tx, ty, z0, z1, sm, dsm);
+        __syncthreads();  // the planes are reused by the next brick
+    });
+}
+
+// Counts the floats x for which fx_div_by_const(x, d, rcp) differs from the IEEE
+// quotient x / d (every bit pattern, 2^32 of them; any NaN matches any NaN).
+__global__ void fxk_check_div(float d, float rcp, unsigned long long* __restrict__ mismatches) {
+    unsigned long long bad = 0;
+    const unsigned long long n = 1ull << 32;
+    for (unsigned long long b = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; b < n;
+         b += (unsigned long long)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float((unsigned)b);
+        const float a = fx_div_by_const(x, d, rcp), e = __fdiv_rn(x, d);
+        bad += (__float_as_uint(a) != __float_as_uint(e)) && !(a != a && e != e);  // NaN == NaN
+    }
+    if (bad) atomicAdd(mismatches, bad);
+}
+
+// ---- single-simulation utilities -----------------------------------------------------------
+// initializeFields (shaders.ts:135-149) plus the seeded velocity noise extension; writes
+// flow[fi] and species[si] of the descriptor.
+template <class St>
+__global__ void fxk_init(const FxSimDev* __restrict__ S, float tAmbient, float oxygen, float noise) {
+    const long long n = (long long)S->X * S->Y * S->Z;
+    void* flow = S->flow[S->fi];
+    void* species = S->species[S->si];
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < n; id += (long long)gridDim.x * blockDim.x) {
+        float4 f = make_float4(0.0f, 0.0f, 0.0f, tAmbient);
+        if (noise > 0.0f) {
+            f.x = fx_velocity_noise(S->seed, (uint64_t)id, 0, noise);
+            f.y = fx_velocity_noise(S->seed, (uint64_t)id, 1, noise);
+            f.z = fx_velocity_noise(S->seed, (uint64_t)id, 2, noise);
+        }
+        fx_st_flow(flow, id, f);
+        St::st_species(species, id, make_float4(0.0f, fx_max(oxygen, 0.0f), 0.0f, 0.0f));
+    }
+}
+
+__global__ void fxk_emitter_mask(const FxSimDev* __restrict__ S, uint8_t* __restrict__ mask) {
+    const long long n = (long long)S->X * S->Y * S->Z;
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < n; id += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(id % S->X);
+        const int y = (int)((id / S->X) % S->Y);
+        const int z = (int)(id / ((long long)S->X * S->Y));
+        uint8_t m = 0;
+        if (S->prm.emitter_mode == FIREX_EMITTER_SPHERES)
+            for (int s = 0; s < S->prm.num_spheres; ++s)
+                if (fx_sphere_inside(S->prm.spheres[s], x, y, z)) m = 1;
+        mask[id] = m;
+    }
+}
+
+// Divergence of the canonical flow F[fi] into out (the FINAL_DIVERGENCE field).
+__global__ void fxk_final_divergence(const FxSimDev* __restrict__ S, float* __restrict__ out) {
+    const long long n = (long long)S->X * S->Y * S->Z;
+    const float3 m = fx_metric(S->prm.u);
+    const void* flow = S->flow[S->fi];
+    const FxGrid g{S->X, S->Y, S->Z};
+    for (long long id = blockIdx.x * (long long)blockDim.x + threadIdx.x; id < n; id += (long long)gridDim.x * blockDim.x) {
+        const int x = (int)(id % S->X);
+        const int y = (int)((id / S->X) % S->Y);
+        const int z = (int)(id / ((long long)S->X * S->Y));
+        const float4 c = fx_ld_flow(flow, id);
+        const float l = fx_ld_flow(flow, g.idx(x - 1, y, z)).x;
+        const float bo = fx_ld_flow(flow, g.idx(x, y - 1, z)).y;
+        const float ba = fx_ld_flow(flow, g.idx(x, y, z - 1)).z;
+        out[id] = (c.x - l) * m.x + (c.y - bo) * m.y + (c.z - ba) * m.z;
+    }
+}
+
+// Post-projection divergence norm over interior cells (the one-cell shell excluded,
+// qualityShaders.ts:47-57): per-block FP64 partial (sum of squares, max abs), then a
+// fixed-order final reduction (deterministic).
+__global__ void __launch_bounds__(256) fxk_norm_partial(const FxSimDev* __restrict__ S, double* __restrict__ partial) {
+    const float3 m = fx_metric(S->prm.u);
+    const void* flow = S->flow[S->fi];
+    const long long X = S->X, XY = (long long)S->X * S->Y;
+    const long long nInt = (long long)(S->X - 2) * (S->Y - 2) * (S->Z - 2);
+    double ss = 0.0, mx = 0.0;
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nInt; k += (long long)gridDim.x * blockDim.x) {
+        const int x = 1 + (int)(k % (S->X - 2));
+        const int y = 1 + (int)((k / (S->X - 2)) % (S->Y - 2));
+        const int z = 1 + (int)(k / ((long long)(S->X - 2) * (S->Y - 2)));
+        const long long id = x + X * y + XY * z;
+        const float4 c = fx_ld_flow(flow, id);
+        const float d = (c.x - fx_ld_flow(flow, id - 1).x) * m.x + (c.y - fx_ld_flow(flow, id - X).y) * m.y +
+                        (c.z - fx_ld_flow(flow, id - XY).z) * m.z;
+        const double dd = (double)d;
+        ss += dd * dd;
+        mx = fmax(mx, fabs(dd));
+    }
+    __shared__ double s_ss[256], s_mx[256];
+    const int t = threadIdx.x;
+    s_ss[t] = ss;
+    s_mx[t] = mx;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w) {
+            s_ss[t] += s_ss[t + w];
+            s_mx[t] = fmax(s_mx[t], s_mx[t + w]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        partial[2 * blockIdx.x] = s_ss[0];
+        partial[2 * blockIdx.x + 1] = s_mx[0];
+    }
+}
+
+__global__ void fxk_norm_final(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
+    __shared__ double s_ss[256], s_mx[256];
+    const int t = threadIdx.x;
+    double ss = 0.0, mx = 0.0;
+    for (int b = t; b < nblocks; b += blockDim.x) {
+        ss += partial[2 * b];
+        mx = fmax(mx, partial[2 * b + 1]);
+    }
+    s_ss[t] = ss;
+    s_mx[t] = mx;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (t < w) {
+            s_ss[t] += s_ss[t + w];
+            s_mx[t] = fmax(s_mx[t], s_mx[t + w]);
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        out[0] = sqrt(s_ss[0]);
+        out[1] = s_mx[0];
+    }
+}
+
+}  // namespace
+
+// ---- launch wrappers ---------------------------------------------------------------------------
+static int g_num_sms = 0;
+static int num_sms() {
+    if (!g_num_sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+        if (g_num_sms <= 0) g_num_sms = 148;
+    }
+    return g_num_sms;
+}
+
+// Grid sizing. Stencil passes launch one CTA per brick (the hardware keeps every SM
+// full and overlaps CTAs' memory latency); FX_PERSISTENT_ROW4 switches them to a
+// persistent grid of full residency that strides over the bricks.
+static int g_row4_persistent = -1;
+static bool row4_persistent() {
+    if (g_row4_persistent < 0) {
+        const char* e = getenv("FX_PERSISTENT_ROW4");
+        g_row4_persistent = (e && e[0] == '1') ? 1 : 0;
+    }
+    return g_row4_persistent == 1;
+}
+static int row4_grid(int g, int bricks) { return row4_persistent() ? (bricks < g ? bricks : g) : bricks; }
+
+// Persistent grid: enough CTAs for full residency, never more than the brick count.
+static int persistent_grid(const void* kernel, int threads, int bricks) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0);
+    if (per_sm <= 0) per_sm = 1;
+    long long g = (long long)per_sm * num_sms();
+    if (bricks > 0 && bricks < g) g = bricks;
+    return (int)(g < 1 ? 1 : g);
+}
+
+void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B) { fxk_step_begin<<<1, 256, 0, s>>>(B); }
+void fx_launch_step_end(cudaStream_t s, FxBatchDev* B) { fxk_step_end<<<1, 256, 0, s>>>(B); }
+
+void fx_launch_simulate(cudaStream_t s, int storage, const FxBatchDev* B, int bricks) {
+    if (storage == FX_STORAGE_MIXED) {
+        static int g = persistent_grid((const void*)fxk_simulate<StMixed>, 256, 1 << 30);
+        fxk_simulate<StMixed><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
+    } else {
+        static int g = persistent_grid((const void*)fxk_simulate<StF32>, 256, 1 << 30);
+        fxk_simulate<StF32><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
+    }
+}
+
+void fx_launch_divergence(cudaStream_t s, const FxBatchDev* B, int bricks, int phase) {
+    static int g = persistent_grid((const void*)fxk_divergence, 256, 1 << 30);
+    fxk_divergence<<<row4_grid(g, bricks), 256, 0, s>>>(B, phase);
+}
+
+void fx_launch_jacobi(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase, int launch, int sweep) {
+    if (half) {
+        static int g = persistent_grid((const void*)fxk_jacobi<__half>, 256, 1 << 30);
+        fxk_jacobi<__half><<<row4_grid(g, bricks), 256, 0, s>>>(B, phase, launch, sweep);
+    } else {
+        static int g = persistent_grid((const void*)fxk_jacobi<float>, 256, 1 << 30);
+        fxk_jacobi<float><<<row4_grid(g, bricks), 256, 0, s>>>(B, phase, launch, sweep);
+    }
+}
+
+template <typename PT>
+static void launch_zm(cudaStream_t s, const FxBatchDev* B, int bricks, int phase, int launch, int sweep, int zc) {
+    static const int g = [] {
+        cudaFuncSetAttribute((const void*)fxk_jacobi_zm<PT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(FxZmSmem<PT>));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fxk_jacobi_zm<PT>, FX_ZM_THREADS,
+                                                      sizeof(FxZmSmem<PT>));
+        return (per_sm > 0 ? per_sm : 1) * num_sms();
+    }();
+    fxk_jacobi_zm<PT><<<row4_grid(g, bricks), FX_ZM_THREADS, sizeof(FxZmSmem<PT>), s>>>(B, phase, launch, sweep, zc);
+}
+
+void fx_launch_jacobi_zm(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase, int launch, int sweep,
+                         int zc) {
+    if (half) launch_zm<__half>(s, B, bricks, phase, launch, sweep, zc);
+    else launch_zm<float>(s, B, bricks, phase, launch, sweep, zc);
+}
+
+template <int K, typename PT, bool ROUND>
+static int tb_grid() {
+    constexpr int smem = fx_tb_smem_bytes(K);
+    cudaFuncSetAttribute((const void*)fxk_jacobi_tb<K, PT, ROUND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fxk_jacobi_tb<K, PT, ROUND>, FX_TB_THREADS, smem);
+    return (per_sm > 0 ? per_sm : 1) * num_sms();
+}
+
+template <int K, typename PT, bool ROUND>
+static void launch_tb(cudaStream_t s, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
+    static int g = tb_grid<K, PT, ROUND>();
+    fxk_jacobi_tb<K, PT, ROUND><<<bricks < g ? bricks : g, FX_TB_THREADS, fx_tb_smem_bytes(K), s>>>(B, phase, launch, zc);
+}
+
+template <int K>
+static void launch_tb_k(cudaStream_t s, int pmode, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
+    if (pmode == FX_TB_F32) launch_tb<K, float, false>(s, B, bricks, phase, launch, zc);
+    else if (pmode == FX_TB_F16_ROUND) launch_tb<K, __half, true>(s, B, bricks, phase, launch, zc);
+    else launch_tb<K, __half, false>(s, B, bricks, phase, launch, zc);
+}
+
+bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
+    switch (k) {
+        case 2: launch_tb_k<2>(s, pmode, B, bricks, phase, launch, zc); return true;
+        case 3: launch_tb_k<3>(s, pmode, B, bricks, phase, launch, zc); return true;
+        case 4: launch_tb_k<4>(s, pmode, B, bricks, phase, launch, zc); return true;
+        case 6: launch_tb_k<6>(s, pmode, B, bricks, phase, launch, zc); return true;
+    }
+    return false;
+}
+
+void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase) {
+    if (half) {
+        static int g = persistent_grid((const void*)fxk_project<__half>, 256, 1 << 30);
+        fxk_project<__half><<<row4_grid(g, bricks), 256, 0, s>>>(B, phase);
+    } else {
+        static int g = persistent_grid((const void*)fxk_project<float>, 256, 1 << 30);
+        fxk_project<float><<<row4_grid(g, bricks), 256, 0, s>>>(B, phase);
+    }
+}
+
+void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbient, float oxygen, float noise) {
+    if (storage == FX_STORAGE_MIXED) fxk_init<StMixed><<<num_sms() * 8, 256, 0, s>>>(S, tAmbient, oxygen, noise);
+    else fxk_init<StF32><<<num_sms() * 8, 256, 0, s>>>(S, tAmbient, oxygen, noise);
+}
+
+void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask) {
+    fxk_emitter_mask<<<num_sms() * 8, 256, 0, s>>>(S, mask);
+}
+
+void fx_launch_final_divergence(cudaStream_t s, const FxSimDev* S, float* out) {
+    fxk_final_divergence<<<num_sms() * 8, 256, 0, s>>>(S, out);
+}
+
+int fx_norm_partial_blocks(long long cells) {
+    long long b = (cells + 255) / 256;
+    const long long cap = 148LL * 8;
+    return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
+}
+
+void fx_launch_divergence_norm(cudaStream_t s, const FxSimDev* S, long long cells, double* partial, double* out) {
+    const int nb = fx_norm_partial_blocks(cells);
+    fxk_norm_partial<<<nb, 256, 0, s>>>(S, partial);
+    fxk_norm_final<<<1, 256, 0, s>>>(partial, nb, out);
+}
+
+// Descriptor uploads travel as kernel arguments: no host staging buffer has to outlive
+// the call, and the copy is ordered on the stream like any other pass.
+namespace {
+__global__ void fxk_upload_desc(FxSimDev v, FxSimDev* __restrict__ dst) {
+    const int* src = reinterpret_cast<const int*>(&v);
+    int* d = reinterpret_cast<int*>(dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(FxSimDev) / 4); i += blockDim.x) d[i] = src[i];
+}
+}  // namespace
+
+void fx_launch_upload_desc(cudaStream_t s, const FxSimDev& host, FxSimDev* dev) { fxk_upload_desc<<<1, 128, 0, s>>>(host, dev); }
+
+void fx_launch_upload_batch(cudaStream_t s, const FxBatchDev& host, FxBatchDev* dev) {
+    // The batch table is larger than a kernel argument: copy the used prefix of each array.
+    cudaMemcpyAsync(dev, &host, sizeof(FxBatchDev), cudaMemcpyHostToDevice, s);
+}
+
+void fx_launch_check_div(cudaStream_t s, float d, float rcp, unsigned long long* mismatches) {
+    fxk_check_div<<<num_sms() * 16, 256, 0, s>>>(d, rcp, mismatches);
+}

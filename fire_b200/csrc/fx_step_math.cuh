@@ -282,7 +282,30 @@ FXD FxJacobiConst fx_jacobi_const(const float* u) {
 
 // One Jacobi update from the six neighbours (shaders.ts:390-402), same order of
 // operations as the reference: ((wx*(l+r) + wy*(b+t)) + wz*(k+f) - div) / denom.
+FXD float fx_jacobi_numerator(const FxJacobiConst& c, float l, float r, float b, float t, float k, float f, float div) {
+    return __fsub_rn(__fadd_rn(__fadd_rn(__fmul_rn(c.wx, __fadd_rn(l, r)), __fmul_rn(c.wy, __fadd_rn(b, t))),
+                               __fmul_rn(c.wz, __fadd_rn(k, f))),
+                     div);
+}
 FXD float fx_jacobi_update(const FxJacobiConst& c, float l, float r, float b, float t, float k, float f, float div) {
-    float nb = c.wx * (l + r) + c.wy * (b + t) + c.wz * (k + f);
-    return (nb - div) / c.denom;
+    return __fdiv_rn(fx_jacobi_numerator(c, l, r, b, t, k, f, div), c.denom);
+}
+
+// Division by a constant d > 0 given rcp = RN(1/d): Markstein's correction step
+// (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): q = RN(x*rcp), e = x - q*d exactly by one
+// fused multiply-add, result RN(q + e*rcp). The theorem assumes no underflow, so the
+// step is used for 2^-96 <= |x| <= FLT_MAX (the quotient stays normal for any d below
+// 2^30); zeros (whose sign must survive) and tiny x take the IEEE division, and
+// x = +-inf or NaN, whose IEEE quotient by a finite d > 0 is x itself, is returned. The
+// engine enables this path for a given d only after checking on the device that it
+// equals IEEE x/d for every float x.
+FXD float fx_div_by_const(float x, float d, float rcp) {
+    const float ax = fabsf(x);
+    if (ax >= 1.2621774483536189e-29f && ax <= 3.402823466e38f) {  // 2^-96 .. FLT_MAX
+        const float q = __fmul_rn(x, rcp);
+        const float e = __fmaf_rn(-q, d, x);
+        return __fmaf_rn(e, rcp, q);
+    }
+    return ax <= 3.402823466e38f ? __fdiv_rn(x, d) : x;
 }

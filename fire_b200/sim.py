@@ -244,6 +244,20 @@ class FireXSim(_Handle):
     def stream(self) -> int:
         return self._lib.firex_stream(self._h) or 0
 
+    def set_jacobi(self, kernel, block: int = 1, zchunk: int = 0) -> None:
+        """Jacobi kernel: 'auto', 'unblocked', 'zmarch' or 'fused' (with `block` sweeps per
+        launch), and z planes per CTA (0 = auto)."""
+        self._check(self._lib.firex_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
+
+    @property
+    def diagnostics(self) -> dict:
+        d = A.Diagnostics()
+        self._check(self._lib.firex_get_diagnostics(self._h, C.byref(d)))
+        return {k: getattr(d, k) for k, _ in A.Diagnostics._fields_ if k != "reserved"}
+
+    def set_graphs(self, on: bool) -> None:
+        self._check(self._lib.firex_set_graphs(self._h, 1 if on else 0))
+
     def set_profiling(self, on: bool) -> None:
         self._check(self._lib.firex_set_profiling(self._h, 1 if on else 0))
 
@@ -253,3 +267,81 @@ class FireXSim(_Handle):
         n = (C.c_int64 * len(A.PASS_NAMES))()
         self._check(self._lib.firex_pass_times(self._h, ms, n))
         return {name: (ms[i], n[i]) for i, name in enumerate(A.PASS_NAMES)}
+
+
+JACOBI_KERNELS = {"auto": A.JACOBI_AUTO, "unblocked": A.JACOBI_UNBLOCKED, "zmarch": A.JACOBI_ZMARCH,
+                  "fused": A.JACOBI_FUSED}
+
+
+def jacobi_kernel(kernel) -> int:
+    return JACOBI_KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+
+
+def planned_device_bytes(dims, options: A.Options) -> int:
+    """Device bytes firex_create would allocate (admission control)."""
+    return int(load_library().firex_planned_device_bytes(A.DIMS(*dims), C.byref(options)))
+
+
+class FireXBatch:
+    """Simulations stepped together by the same launches (firex_batch_*).
+
+    Members may have different grid sizes and iteration counts; they must share the
+    storage precision and the pressure storage type. While a member, a simulation is
+    stepped only through the batch; its reads and writes stay valid.
+    """
+
+    def __init__(self):
+        self._lib = load_library()
+        self._h = C.c_void_p()
+        rc = self._lib.firex_batch_create(C.byref(self._h))
+        if rc != A.OK:
+            raise FireXError(rc, (self._lib.firex_batch_last_error(None) or b"").decode())
+        self.members: list[FireXSim] = []
+
+    def _check(self, rc: int) -> None:
+        if rc != A.OK:
+            raise FireXError(rc, (self._lib.firex_batch_last_error(self._h) or b"").decode())
+
+    def add(self, sim: FireXSim) -> None:
+        self._check(self._lib.firex_batch_add(self._h, sim._h))
+        self.members.append(sim)
+
+    def remove(self, sim: FireXSim) -> None:
+        self._check(self._lib.firex_batch_remove(self._h, sim._h))
+        self.members.remove(sim)
+
+    def __len__(self) -> int:
+        n = C.c_int32()
+        self._check(self._lib.firex_batch_size(self._h, C.byref(n)))
+        return n.value
+
+    def step(self, n: int = 1, dt: float = 1.0 / 60.0) -> None:
+        self._check(self._lib.firex_batch_step(self._h, int(n), float(dt)))
+
+    def set_jacobi(self, kernel, block: int = 1, zchunk: int = 0) -> None:
+        self._check(self._lib.firex_batch_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
+
+    def sync(self) -> None:
+        self._check(self._lib.firex_batch_sync(self._h))
+
+    @property
+    def stream(self) -> int:
+        return self._lib.firex_batch_stream(self._h) or 0
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.firex_batch_destroy(self._h)
+            self._h = C.c_void_p()
+            self.members = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -81,9 +81,10 @@ typedef struct firex_options {
     float velocity_noise;          /* initial velocity: uniform in [-a, a] per component */
     float emission_jitter;         /* per-step emission factor uniform in [1-a, 1+a] */
     int32_t cinematic;             /* mixing.z; offline tiers force 1 (FireXEngine.ts:2097,2819) */
-    int32_t jacobi_block;          /* sweeps fused per Jacobi launch (temporal block); 0 = auto */
+    int32_t jacobi_block;          /* > 1: fuse this many Jacobi sweeps per launch (see firex_set_jacobi) */
     uint64_t memory_budget_bytes;  /* 0 = no budget; else create fails with FIREX_ERR_BUDGET */
-    int32_t reserved[8];
+    int32_t jacobi_zchunk;         /* z planes per CTA of a fused Jacobi launch; 0 = auto */
+    int32_t reserved[7];
 } firex_options;
 
 /* Fills *opt with the defaults: F32, AUTO pressure, P = R = 64 (offline HD tier,
@@ -119,6 +120,7 @@ typedef struct firex_state {
 #define FIREX_UNIFORM_FLOATS 44  /* FireXEngine.ts:163 */
 
 typedef struct firex_sim firex_sim;
+typedef struct firex_batch firex_batch;
 
 /* Allocates the solver bundle for a dims[0] x dims[1] x dims[2] grid and resets it.
  * Axes must be positive multiples of 4 (gridConfiguration.ts:98, preflight :306-317).
@@ -204,6 +206,58 @@ int firex_set_profiling(firex_sim* sim, int32_t on);
  * pass (ms[FIREX_PASS_COUNT]) and the number of kernel launches per pass
  * (launches[FIREX_PASS_COUNT]) since the previous call. Either pointer may be NULL. */
 int firex_pass_times(firex_sim* sim, double* ms, int64_t* launches);
+
+/* Device bytes firex_create would allocate for this grid and options (admission). */
+uint64_t firex_planned_device_bytes(const int32_t dims[3], const firex_options* opt);
+
+/* Replays each step from a captured CUDA graph (1, the default) or launches the passes
+ * directly (0). Results are identical; graphs remove per-launch host overhead. */
+int firex_set_graphs(firex_sim* sim, int32_t on);
+
+/* Jacobi kernel choice. Every kernel computes each sweep's update with the same FP32
+ * operations; they differ in how data reaches the SMs:
+ *   UNBLOCKED — one thread per 4 cells, neighbours through L1 (best for small grids);
+ *   ZMARCH    — x-y tiles marching z through a cp.async shared-memory ring (one read of
+ *               each value per sweep: best once the grid outgrows L2);
+ *   FUSED     — `block` sweeps per launch (2, 3, 4 or 6), temporally blocked. Fused sweeps
+ *               give the same results as single sweeps except that mixed precision keeps
+ *               the intermediate sweeps in FP32. A phase falls back to single sweeps when
+ *               fusing would change which buffer holds the result.
+ * `zchunk`: z planes per CTA for ZMARCH and FUSED (0 = auto). AUTO picks by grid size. */
+#define FIREX_JACOBI_AUTO 0
+#define FIREX_JACOBI_UNBLOCKED 1
+#define FIREX_JACOBI_ZMARCH 2
+#define FIREX_JACOBI_FUSED 3
+int firex_set_jacobi(firex_sim* sim, int32_t kernel, int32_t block, int32_t zchunk);
+int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, int32_t zchunk);
+
+/* What the engine chose for the most recent step of the simulation (or its batch). */
+typedef struct firex_diagnostics {
+    int32_t fast_division;    /* 1: the Jacobi division uses the checked constant-divisor path */
+    int32_t jacobi_block;     /* sweeps fused per Jacobi launch (1: one sweep per launch) */
+    int32_t jacobi_zchunk;    /* z planes per CTA of the Jacobi launches */
+    int32_t graph;            /* 1: steps replay a captured CUDA graph */
+    int32_t launches_per_step;
+    int32_t reserved[11];
+} firex_diagnostics;
+int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
+
+/* ---- batches: many simulations stepped by the same launches -------------------------
+ * No reference counterpart (the reference runs one simulation per WebGPU device). A batch
+ * steps its members together: each pass is one persistent launch over the bricks of all
+ * members, whatever their grid sizes, and the step is replayed from a CUDA graph. Members
+ * must share the storage precision and the pressure storage type; their iteration counts
+ * may differ. While a member, a simulation is stepped only through its batch; its field,
+ * parameter and state calls stay valid and are ordered with the batch's work. */
+int firex_batch_create(firex_batch** out);
+int firex_batch_destroy(firex_batch* batch); /* members are detached, not destroyed */
+int firex_batch_add(firex_batch* batch, firex_sim* sim);
+int firex_batch_remove(firex_batch* batch, firex_sim* sim);
+int firex_batch_size(const firex_batch* batch, int32_t* members);
+int firex_batch_step(firex_batch* batch, int32_t nsteps, double dt);
+int firex_batch_sync(firex_batch* batch);
+const char* firex_batch_last_error(const firex_batch* batch);
+void* firex_batch_stream(const firex_batch* batch);
 
 #ifdef __cplusplus
 }

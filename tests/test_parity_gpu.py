@@ -26,9 +26,12 @@ from tests.helpers import DT, burner_options, copy_state, max_abs, rel_l2, spher
 
 pytestmark = pytest.mark.gpu
 
-ATOL = {"flow_uvw": 2e-5, "flow_T": 2e-3, "species": 2e-5, "reaction": 2e-5, "pressure_rel": 2e-5}
-REL_FIELD = 2e-3
-REL_NORM = 2e-3
+# Observed on B200 (max over cases): flow_uvw 3e-8, flow_T 3.1e-4 (1 ULP at ~2000 K),
+# species 1.8e-7, reaction 3.8e-7, pressure_rel 2.7e-7; 60-step config 1: 1.5e-5 (flow),
+# 2.9e-5 (pressure), 2.3e-5 (divergence norm).
+ATOL = {"flow_uvw": 1e-6, "flow_T": 2e-3, "species": 2e-6, "reaction": 4e-6, "pressure_rel": 4e-6}
+REL_FIELD = 3e-4
+REL_NORM = 3e-4
 
 REPORT = os.environ.get("FIREX_PARITY_REPORT")
 
@@ -89,7 +92,7 @@ def test_uniform_block_bit_exact():
     assert g.state == o.state
 
 
-@pytest.mark.parametrize("mode", [A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32])
+@pytest.mark.parametrize("mode", [A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32, A.PRESSURE_F16])
 @pytest.mark.parametrize("dims", [(16, 20, 24), (64, 96, 64)])
 def test_zero_dt_sphere_steps_bit_exact(dims, mode):
     """dt = 0 removes every transcendental from the step's results: the divergence,
@@ -207,3 +210,18 @@ def test_budget_and_bad_dims_are_refused():
     with pytest.raises(FireXError) as e:
         FireXSim((62, 96, 64), make_options())
     assert e.value.code == A.ERR_BAD_ARG
+
+
+@pytest.mark.parametrize("R", [0, 1, 2])
+@pytest.mark.parametrize("P", [0, 1, 2])
+def test_small_iteration_counts_bit_exact(P, R):
+    """Ping-pong parity, zero-input first sweeps and the cleared buffers the reference
+    leaves behind (FireXEngine.ts:2215-2230, 2258-2259) for P, R in {0, 1, 2}."""
+    dims = (16, 20, 24)
+    for mode in (A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32, A.PRESSURE_F16):
+        opts = sphere_options(dims, P=P, R=R, pressure_mode=mode)
+        g, o = FireXSim(dims, opts), OracleSim(dims, opts)
+        g.step(3, 0.0)
+        o.step(3, 0.0)
+        assert g.state == o.state, mode
+        fields_equal(g, o)
