@@ -14,6 +14,28 @@
 
 #include "../../include/firex.h"
 
+// Constant divisors of simulate. Each slot holds d > 0, rcp = RN(1/d) and the range
+// [lo, hi] of |x| where Markstein's correction step (fx_div_checked) reproduces IEEE
+// x / d; ok = 1 once the engine has checked that on the device for every float x.
+struct FxDivc {
+    float d, rcp, lo, hi;
+    int ok, pad[3];
+};
+enum FxDivSlot {
+    DIVC_SIX = 0,        // the 6-neighbour averages (shaders.ts:177-186)
+    DIVC_FUELCORE,       // smoothstep(0.30, 0.78, fuel)
+    DIVC_ENTRAIN_T,      // smoothstep(400, 1500, T)
+    DIVC_IGNITION,       // smoothstep(690, 930, T)
+    DIVC_HOTPLUME,       // smoothstep(520, 1650, T)
+    DIVC_EVAP,           // smoothstep(335, 1040, T)
+    DIVC_LOBE,           // smoothstep(-0.42, 0.48, lobe)
+    DIVC_BUOYANCY,       // (T - T_amb) / 1500
+    DIVC_AMBIENT_O2,     // (ambientOxygen - O2) / ambientOxygen
+    DIVC_DT,             // burn / max(dt, 0.0001)
+    DIVC_RADIATION,      // ... / (1005 * persistence)
+    DIVC_COUNT
+};
+
 // Per-step parameter block: the reference's 44-float uniform block (shaders.ts:2-14,
 // written by FireXEngine.writeUniforms, FireXEngine.ts:2043-2113) followed by the
 // sphere-emitter extension.
@@ -57,13 +79,14 @@ FXD float fx_length3(float x, float y, float z) { return sqrtf(x * x + y * y + z
 // Float constant rounded from its double literal, as WGSL concretises abstract floats.
 #define FC(v) (static_cast<float>(v))
 
+// Grids hold fewer than 2^31 cells, so 32-bit cell offsets are exact.
 struct FxGrid {
     int X, Y, Z;
-    __device__ __forceinline__ long long idx(int x, int y, int z) const {
+    __device__ __forceinline__ int idx(int x, int y, int z) const {
         x = x < 0 ? 0 : (x > X - 1 ? X - 1 : x);
         y = y < 0 ? 0 : (y > Y - 1 ? Y - 1 : y);
         z = z < 0 ? 0 : (z > Z - 1 ? Z - 1 : z);
-        return (long long)x + (long long)X * ((long long)y + (long long)Y * (long long)z);
+        return x + X * (y + Y * z);
     }
 };
 
@@ -138,17 +161,20 @@ struct __align__(16) FxSimDev {
     float* div;
     float* reaction;
     uint32_t* liquid;
+    float* tab;            // per-step tables of simulate (fx_step_math.cuh)
+    FxDivc divc[DIVC_COUNT];
 };
 
 // Work decomposition shared by every batched pass: each pass walks a flat list of
 // bricks across all simulations of a batch; start[shape][s] is the first brick of
 // simulation s (prefix sums over the batch), so one launch covers uneven grids.
 #define FX_MAX_BATCH 512
-enum FxShape { FX_SHAPE_CELL = 0, FX_SHAPE_ROW4 = 1, FX_SHAPE_COL = 2, FX_SHAPE_ZM = 3, FX_NSHAPES = 4 };
+enum FxShape { FX_SHAPE_CELL = 0, FX_SHAPE_ROW4 = 1, FX_SHAPE_COL = 2, FX_SHAPE_ZM = 3, FX_SHAPE_TAB = 4, FX_NSHAPES = 5 };
 // CELL: 32 x 4 x 2 cells, one thread per cell (simulate).
 // ROW4: 256 groups of 4 consecutive x cells in memory order (stencils).
 // COL : column tiles of the temporally blocked Jacobi (see fx_jacobi_tb.cuh).
 // ZM  : z-marching tiles of the single-sweep Jacobi (see fx_jacobi_zm.cuh).
+// TAB : 256 entries of the per-step tables of simulate.
 #define FX_CELL_BX 32
 #define FX_CELL_BY 4
 #define FX_CELL_BZ 2

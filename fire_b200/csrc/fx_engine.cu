@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <tuple>
@@ -126,10 +127,10 @@ struct StepPlan {
     int zmZc = 16;            // z planes per CTA of the single-sweep (z-marching) kernel
     bool row4 = false;        // single sweeps by the unblocked kernel instead
     bool fuseP = false, fuseR = false;
-    int bricks[FX_NSHAPES] = {0, 0, 0, 0};
+    int bricks[FX_NSHAPES] = {0, 0, 0, 0, 0};
     auto key() const {
         return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, bricks[0], bricks[1], bricks[2],
-                        bricks[3]);
+                        bricks[3], bricks[4]);
     }
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
 };
@@ -161,6 +162,7 @@ void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, in
 
 void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     fx_launch_step_begin(st, B);
+    fx_launch_step_tables(st, B, pl.bricks[FX_SHAPE_TAB]);
     fx_launch_simulate(st, pl.storage, B, pl.bricks[FX_SHAPE_CELL]);
     fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 0);
     enqueue_jacobi_phase(st, pl, B, 0);
@@ -193,11 +195,16 @@ struct firex_batch;
 // Whether fx_div_by_const(x, d, rcp) equals IEEE x / d for every finite float x on this
 // device, checked once per (device, d) by fxk_check_div (about a millisecond). Results
 // are cached for the life of the process. Any CUDA error answers "no".
-static bool fast_division_ok(int device, float d, float rcp) {
-    static std::map<std::pair<int, uint32_t>, bool> cache;
-    uint32_t bits;
+static bool fast_division_ok(int device, float d, float rcp, float lo = 1.2621774483536189e-29f,
+                             float hi = 3.402823466e38f) {
+    static std::map<std::tuple<int, uint32_t, uint32_t, uint32_t>, bool> cache;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    uint32_t bits, lb, hb;
     std::memcpy(&bits, &d, 4);
-    auto key = std::make_pair(device, bits);
+    std::memcpy(&lb, &lo, 4);
+    std::memcpy(&hb, &hi, 4);
+    auto key = std::make_tuple(device, bits, lb, hb);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
     bool ok = false;
@@ -206,7 +213,7 @@ static bool fast_division_ok(int device, float d, float rcp) {
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
         cudaMalloc(&dcount, sizeof(unsigned long long)) == cudaSuccess &&
         cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), st) == cudaSuccess) {
-        fx_launch_check_div(st, d, rcp, dcount);
+        fx_launch_check_div(st, d, rcp, lo, hi, dcount);
         unsigned long long bad = ~0ull;
         if (cudaMemcpyAsync(&bad, dcount, sizeof(bad), cudaMemcpyDeviceToHost, st) == cudaSuccess &&
             cudaStreamSynchronize(st) == cudaSuccess)
@@ -270,12 +277,15 @@ struct firex_sim {
         return p;
     }
 
-    static size_t planned_bytes(long long N, int storage, int mode) {
+    static size_t planned_bytes(int X, int Y, int Z, int storage, int mode) {
+        const long long N = (long long)X * Y * Z;
         const size_t species = storage == FX_STORAGE_MIXED ? 8 : 16;
         const size_t pbytes = (storage == FX_STORAGE_MIXED || mode == FIREX_PRESSURE_F16) ? 2 : 4;
         const size_t npress = mode == FIREX_PRESSURE_COLD_F32 ? 2 : 4;
         const size_t per = 16 * 2 + species * 2 + pbytes * npress + 4 /*div*/ + 4 /*reaction*/ + 4 /*liquid*/ + 4 /*tmp*/;
-        return (size_t)N * per + sizeof(FxSimDev) + 64 * 1024;
+        return (size_t)N * per + (size_t)fx_tab_layout(X, Y, Z).total * 4 + sizeof(FxSimDev) + 64 * 1024;
+    }
+    size_t table_bytes() const { return (size_t)fx_tab_layout(X, Y, Z).total * 4;
     }
 
     size_t species_bytes() const { return storage == FX_STORAGE_MIXED ? 8 : 16; }
@@ -322,6 +332,25 @@ struct firex_sim {
         h.jc[3] = 2.0f * (h.jc[0] + h.jc[1] + h.jc[2]);
         h.jcRcp = 1.0f / h.jc[3];
         h.jcFastDiv = fast_division_ok(device, h.jc[3], h.jcRcp) ? 1 : 0;
+        // constant divisors of simulate, computed with the same f32 operations as the
+        // expressions they stand for
+        auto fmaxr = [](float a, float b) { return (a < b) ? b : a; };
+        auto fminr = [](float a, float b) { return (b < a) ? b : a; };
+        const float persistence = fminr(fmaxr(u[38], 0.4f), 3.0f);
+        const float divisors[DIVC_COUNT] = {
+            6.0f, 0.78f - 0.30f, 1500.0f - 400.0f, 930.0f - 690.0f, 1650.0f - 520.0f, 1040.0f - 335.0f,
+            0.48f - (-0.42f), 1500.0f, fmaxr(u[9], 0.001f), fmaxr(u[4], 0.0001f), 1005.0f * persistence};
+        for (int k = 0; k < DIVC_COUNT; ++k) {
+            FxDivc& c = h.divc[k];
+            std::memset(&c, 0, sizeof(c));
+            c.d = divisors[k];
+            c.rcp = 1.0f / c.d;
+            c.lo = 1.2621774483536189e-29f;  // 2^-96: quotients stay normal for d < 2^30
+            c.hi = (float)std::min(3.4028234663852886e38, 3.4028234663852886e38 * std::min(1.0, (double)c.d) * 0.5);
+            // dt may change every call: its divisor keeps the IEEE division rather than
+            // paying the device check per new value
+            c.ok = (k != DIVC_DT && c.d > 0.0f && c.d < 1073741824.0f && fast_division_ok(device, c.d, c.rcp, c.lo, c.hi)) ? 1 : 0;
+        }
         dirty = true;
     }
 
@@ -385,7 +414,7 @@ struct firex_batch {
 
     // Fills the brick prefix sums for the launch shape (k, zc).
     void fill_table(int k, int zc, int zmZc) {
-        int acc[FX_NSHAPES] = {0, 0, 0, 0};
+        int acc[FX_NSHAPES] = {0, 0, 0, 0, 0};
         h->nsims = (int)members.size();
         for (size_t i = 0; i < members.size(); ++i) {
             firex_sim* s = members[i];
@@ -394,6 +423,8 @@ struct firex_batch {
             h->start[FX_SHAPE_ROW4][i] = acc[FX_SHAPE_ROW4];
             h->start[FX_SHAPE_COL][i] = acc[FX_SHAPE_COL];
             h->start[FX_SHAPE_ZM][i] = acc[FX_SHAPE_ZM];
+            h->start[FX_SHAPE_TAB][i] = acc[FX_SHAPE_TAB];
+            acc[FX_SHAPE_TAB] += (fx_tab_layout(s->X, s->Y, s->Z).total + 255) / 256;
             acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z);
             acc[FX_SHAPE_ROW4] += (int)bricks_row4(s->X, s->Y, s->Z);
             acc[FX_SHAPE_COL] += k > 1 ? fx_tb_bricks(s->X, s->Y, s->Z, k, zc) : 0;
@@ -491,7 +522,8 @@ struct firex_batch {
     void enqueue_profiled(const StepPlan& pl) {
         mark(-1, 0);
         fx_launch_step_begin(stream, d);
-        mark(FIREX_PASS_OTHER, 1);
+        fx_launch_step_tables(stream, d, pl.bricks[FX_SHAPE_TAB]);
+        mark(FIREX_PASS_OTHER, 2);
         fx_launch_simulate(stream, pl.storage, d, pl.bricks[FX_SHAPE_CELL]);
         mark(FIREX_PASS_SIMULATE, 1);
         fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 0);
@@ -562,7 +594,7 @@ struct firex_batch {
             if (e != cudaSuccess) return poison(e, "step");
             for (firex_sim* s : members) s->advance_mirror();
             if (!profiling) {
-                pendingLaunches[FIREX_PASS_OTHER] += 2;
+                pendingLaunches[FIREX_PASS_OTHER] += 3;
                 pendingLaunches[FIREX_PASS_SIMULATE] += 1;
                 pendingLaunches[FIREX_PASS_DIVERGENCE] += 2;
                 pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
@@ -720,7 +752,7 @@ uint64_t firex_planned_device_bytes(const int32_t dims[3], const firex_options* 
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
     const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
-    return firex_sim::planned_bytes(N, storage, mode);
+    return firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode);
 }
 
 int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** out) {
@@ -756,7 +788,7 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         g_create_error = "mixed precision stores pressure in FP16; the cold f32 branch does not apply";
         return FIREX_ERR_UNSUPPORTED;
     }
-    const size_t need = firex_sim::planned_bytes(N, storage, mode);
+    const size_t need = firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode);
     if (opt->memory_budget_bytes && need > opt->memory_budget_bytes) {
         g_create_error = "grid needs " + std::to_string(need) + " device bytes, above the " +
                          std::to_string(opt->memory_budget_bytes) + "-byte budget";
@@ -817,6 +849,7 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
     }
     ok = ok && (h.div = (float*)s->alloc((size_t)N * 4)) && (h.reaction = (float*)s->alloc((size_t)N * 4)) &&
          (h.liquid = (uint32_t*)s->alloc((size_t)N * 4)) && (s->d_tmp = s->alloc((size_t)N * 4)) &&
+         (h.tab = (float*)s->alloc(s->table_bytes())) &&
          (s->d = (FxSimDev*)s->alloc(sizeof(FxSimDev))) &&
          (s->d_partial = (double*)s->alloc(2 * sizeof(double) * (size_t)fx_norm_partial_blocks(N))) &&
          (s->d_norm = (double*)s->alloc(2 * sizeof(double)));
@@ -1091,7 +1124,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_block = p.k;
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
-    out->launches_per_step = 7 + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+    out->launches_per_step = 8 + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
     return FIREX_OK;
 }
 

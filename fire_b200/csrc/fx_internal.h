@@ -12,6 +12,7 @@
 // pass's shape; grids are persistent (full residency) capped at that total.
 void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B);
 void fx_launch_step_end(cudaStream_t s, FxBatchDev* B);
+void fx_launch_step_tables(cudaStream_t s, const FxBatchDev* B, int bricks);
 void fx_launch_simulate(cudaStream_t s, int storage, const FxBatchDev* B, int bricks);
 void fx_launch_divergence(cudaStream_t s, const FxBatchDev* B, int bricks, int phase);
 void fx_launch_jacobi(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase, int launch, int sweep);
@@ -33,4 +34,4 @@ void fx_launch_upload_desc(cudaStream_t s, const FxSimDev& host, FxSimDev* dev);
 void fx_launch_upload_batch(cudaStream_t s, const FxBatchDev& host, FxBatchDev* dev);
 
 // Exhaustive check of fx_div_by_const against IEEE division for one denominator.
-void fx_launch_check_div(cudaStream_t s, float d, float rcp, unsigned long long* mismatches);
+void fx_launch_check_div(cudaStream_t s, float d, float rcp, float lo, float hi, unsigned long long* mismatches);

@@ -76,13 +76,13 @@ struct Acc {
     const void* flowIn;
     const void* speciesIn;
     const uint32_t* liq;
-    FXD float4 flow(long long i) const { return fx_ld_flow(flowIn, i); }
-    FXD float4 species(long long i) const { return St::ld_species(speciesIn, i); }
-    FXD uint32_t liquid(long long i) const { return __ldg(liq + i); }
+    FXD float4 flow(int i) const { return fx_ld_flow(flowIn, i); }
+    FXD float4 species(int i) const { return St::ld_species(speciesIn, i); }
+    FXD uint32_t liquid(int i) const { return __ldg(liq + i); }
 };
 
 template <class St>
-__global__ void __launch_bounds__(256) fxk_simulate(const FxBatchDev* __restrict__ B) {
+__global__ void __launch_bounds__(256, 3) fxk_simulate(const FxBatchDev* __restrict__ B) {
     fx_for_bricks<FX_SHAPE_CELL>(B, [&](const FxSimDev& S, int b) {
         const int nbx = (S.X + FX_CELL_BX - 1) / FX_CELL_BX, nby = (S.Y + FX_CELL_BY - 1) / FX_CELL_BY;
         const int x = (b % nbx) * FX_CELL_BX + threadIdx.x % FX_CELL_BX;
@@ -91,11 +91,19 @@ __global__ void __launch_bounds__(256) fxk_simulate(const FxBatchDev* __restrict
         if (x >= S.X || y >= S.Y || z >= S.Z) return;
         const FxGrid g{S.X, S.Y, S.Z};
         Acc<St> a{S.flow[S.fi], S.species[S.si], S.liquid};
-        FxCellOut o = fx_simulate_cell(S.prm, g, x, y, z, a);
-        const long long id = (long long)x + (long long)S.X * ((long long)y + (long long)S.Y * z);
+        FxCellOut o = fx_simulate_cell(S.prm, g, x, y, z, a, S.tab, S.divc);
+        const int id = x + S.X * (y + S.Y * z);
         fx_st_flow(S.flow[S.fi ^ 1], id, o.flow);
         St::st_species(S.species[S.si ^ 1], id, o.species);
         S.reaction[id] = o.reaction;
+    });
+}
+
+// Per-step tables of simulate (fx_table_entry), after fxk_step_begin set the time fields.
+__global__ void __launch_bounds__(256) fxk_step_tables(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_TAB>(B, [&](const FxSimDev& S, int b) {
+        const int i = b * 256 + (int)threadIdx.x;
+        if (i < fx_tab_layout(S.X, S.Y, S.Z).total) S.tab[i] = fx_table_entry(S.prm.u, S.X, S.Y, S.Z, i);
     });
 }
 
@@ -328,13 +336,13 @@ __global__ void __launch_bounds__(FX_TB_THREADS, 1) fxk_jacobi_tb(const FxBatchD
 
 // Counts the floats x for which fx_div_by_const(x, d, rcp) differs from the IEEE
 // quotient x / d (every bit pattern, 2^32 of them; any NaN matches any NaN).
-__global__ void fxk_check_div(float d, float rcp, unsigned long long* __restrict__ mismatches) {
+__global__ void fxk_check_div(float d, float rcp, float lo, float hi, unsigned long long* __restrict__ mismatches) {
     unsigned long long bad = 0;
     const unsigned long long n = 1ull << 32;
     for (unsigned long long b = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; b < n;
          b += (unsigned long long)gridDim.x * blockDim.x) {
         const float x = __uint_as_float((unsigned)b);
-        const float a = fx_div_by_const(x, d, rcp), e = __fdiv_rn(x, d);
+        const float a = fx_div_range(x, d, rcp, lo, hi), e = __fdiv_rn(x, d);
         bad += (__float_as_uint(a) != __float_as_uint(e)) && !(a != a && e != e);  // NaN == NaN
     }
     if (bad) atomicAdd(mismatches, bad);
@@ -494,6 +502,9 @@ static int persistent_grid(const void* kernel, int threads, int bricks) {
 
 void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B) { fxk_step_begin<<<1, 256, 0, s>>>(B); }
 void fx_launch_step_end(cudaStream_t s, FxBatchDev* B) { fxk_step_end<<<1, 256, 0, s>>>(B); }
+void fx_launch_step_tables(cudaStream_t s, const FxBatchDev* B, int bricks) {
+    fxk_step_tables<<<bricks > 0 ? bricks : 1, 256, 0, s>>>(B);
+}
 
 void fx_launch_simulate(cudaStream_t s, int storage, const FxBatchDev* B, int bricks) {
     if (storage == FX_STORAGE_MIXED) {
@@ -623,6 +634,6 @@ void fx_launch_upload_batch(cudaStream_t s, const FxBatchDev& host, FxBatchDev* 
     cudaMemcpyAsync(dev, &host, sizeof(FxBatchDev), cudaMemcpyHostToDevice, s);
 }
 
-void fx_launch_check_div(cudaStream_t s, float d, float rcp, unsigned long long* mismatches) {
-    fxk_check_div<<<num_sms() * 16, 256, 0, s>>>(d, rcp, mismatches);
+void fx_launch_check_div(cudaStream_t s, float d, float rcp, float lo, float hi, unsigned long long* mismatches) {
+    fxk_check_div<<<num_sms() * 16, 256, 0, s>>>(d, rcp, lo, hi, mismatches);
 }

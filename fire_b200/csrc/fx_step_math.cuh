@@ -10,48 +10,190 @@
 
 #include "fx_device.cuh"
 
+// Division by a constant d > 0 given rcp = RN(1/d): Markstein's correction step
+// (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): q = RN(x*rcp), e = x - q*d exactly by one
+// fused multiply-add, result RN(q + e*rcp). The theorem assumes no underflow, so the
+// step is used for 2^-96 <= |x| <= FLT_MAX (the quotient stays normal for any d below
+// 2^30); zeros (whose sign must survive) and tiny x take the IEEE division, and
+// x = +-inf or NaN, whose IEEE quotient by a finite d > 0 is x itself, is returned. The
+// engine enables this path for a given d only after checking on the device that it
+// equals IEEE x/d for every float x.
+FXD float fx_div_by_const(float x, float d, float rcp) {
+    const float ax = fabsf(x);
+    if (ax >= 1.2621774483536189e-29f && ax <= 3.402823466e38f) {  // 2^-96 .. FLT_MAX
+        const float q = __fmul_rn(x, rcp);
+        const float e = __fmaf_rn(-q, d, x);
+        return __fmaf_rn(e, rcp, q);
+    }
+    return ax <= 3.402823466e38f ? __fdiv_rn(x, d) : x;
+}
+
+// The same step on an explicit range [lo, hi] of |x| (divisors below 1 need hi < FLT_MAX
+// so that x * rcp cannot overflow); outside it IEEE division, or x for inf and NaN.
+FXD float fx_div_range(float x, float d, float rcp, float lo, float hi) {
+    const float ax = fabsf(x);
+    if (ax >= lo && ax <= hi) {
+        const float q = __fmul_rn(x, rcp);
+        const float e = __fmaf_rn(-q, d, x);
+        return __fmaf_rn(e, rcp, q);
+    }
+    return ax <= 3.402823466e38f ? __fdiv_rn(x, d) : x;
+}
+
+// x / c.d, by the checked constant-divisor path when the engine enabled it.
+FXD float fx_divc(float x, const FxDivc& c) { return c.ok ? fx_div_range(x, c.d, c.rcp, c.lo, c.hi) : __fdiv_rn(x, c.d); }
+
+// smoothstep with its constant denominator e1 - e0 held in c.
+FXD float fx_smoothstep_c(float e0, float x, const FxDivc& c) {
+    float t = fx_clamp(fx_divc(x - e0, c), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
 // trilinearFlow / trilinearSpecies (shaders.ts:61-95): 8-tap trilinear sample at
-// position - 0.5, clamped to [0, dims - 1.001]; taps use clamped addressing.
-template <class Load>
-FXD float4 fx_trilinear(const FxGrid& g, const float* u, float px, float py, float pz, Load load) {
+// position - 0.5, clamped to [0, dims - 1.001]. The clamp bounds floor() to
+// [0, dims - 2], so base + 1 is always inside the grid and the reference's clamped tap
+// addressing reduces to fixed offsets (the integer clamp below only guards addresses).
+struct FxTri {
+    int base;
+    float fx, fy, fz;
+};
+FXD FxTri fx_tri_setup(const FxGrid& g, const float* u, float px, float py, float pz) {
     float sx = fx_clamp(px - 0.5f, 0.0f, u[U_GRID_X] - FC(1.001));
     float sy = fx_clamp(py - 0.5f, 0.0f, u[U_GRID_Y] - FC(1.001));
     float sz = fx_clamp(pz - 0.5f, 0.0f, u[U_GRID_Z] - FC(1.001));
     float flx = floorf(sx), fly = floorf(sy), flz = floorf(sz);
-    int bx = (int)flx, by = (int)fly, bz = (int)flz;
-    float fx = sx - flx, fy = sy - fly, fz = sz - flz;
-    float4 c000 = load(g.idx(bx, by, bz)), c100 = load(g.idx(bx + 1, by, bz));
-    float4 c010 = load(g.idx(bx, by + 1, bz)), c110 = load(g.idx(bx + 1, by + 1, bz));
-    float4 c001 = load(g.idx(bx, by, bz + 1)), c101 = load(g.idx(bx + 1, by, bz + 1));
-    float4 c011 = load(g.idx(bx, by + 1, bz + 1)), c111 = load(g.idx(bx + 1, by + 1, bz + 1));
-    float4 z0 = fx_mix4(fx_mix4(c000, c100, fx), fx_mix4(c010, c110, fx), fy);
-    float4 z1 = fx_mix4(fx_mix4(c001, c101, fx), fx_mix4(c011, c111, fx), fy);
-    return fx_mix4(z0, z1, fz);
+    const int bx = min(max((int)flx, 0), g.X - 2), by = min(max((int)fly, 0), g.Y - 2), bz = min(max((int)flz, 0), g.Z - 2);
+    FxTri t;
+    t.base = bx + g.X * (by + g.Y * bz);
+    t.fx = sx - flx;
+    t.fy = sy - fly;
+    t.fz = sz - flz;
+    return t;
+}
+template <class Load>
+FXD float4 fx_trilinear(const FxGrid& g, const FxTri& t, Load load) {
+    const int X = g.X, XY = g.X * g.Y, b = t.base;
+    float4 c000 = load(b), c100 = load(b + 1), c010 = load(b + X), c110 = load(b + X + 1);
+    float4 c001 = load(b + XY), c101 = load(b + XY + 1), c011 = load(b + XY + X), c111 = load(b + XY + X + 1);
+    float4 z0 = fx_mix4(fx_mix4(c000, c100, t.fx), fx_mix4(c010, c110, t.fx), t.fy);
+    float4 z1 = fx_mix4(fx_mix4(c001, c101, t.fx), fx_mix4(c011, c111, t.fx), t.fy);
+    return fx_mix4(z0, z1, t.fz);
 }
 
-// emitter (shaders.ts:101-133): analytic elliptical-Gaussian burner with cellular,
-// lobe and pulse texture, at normalised position (nx, ny, nz).
-FXD float fx_burner(const float* u, float nx, float ny, float nz) {
-    float time = u[U_TIME];
-    float3 ext = fx_extent(u);
-    float px = nx * ext.x, py = ny * ext.y, pz = nz * ext.z;
-    float cx = ext.x * 0.5f + sinf(time * FC(1.73)) * FC(0.013);
-    float cy = FC(0.075);
-    float cz = ext.z * 0.5f + cosf(time * FC(1.37)) * FC(0.011);
-    float ox = px - cx, oy = py - cy, oz = pz - cz;
+// ---- per-step tables ------------------------------------------------------------------------
+// Terms of simulate that depend only on time and on one or two coordinates are computed
+// once per step into a per-simulation table by fxk_step_tables, with the same device
+// expressions the per-cell code would evaluate (so results are bit-identical):
+//   uniform : exp(-dt*0.075/persistence), exp(-dt*0.14/persistence), pow(T_amb, 4)
+//   x       : swirl z term, burner cellular/lobe/radial x terms
+//   y       : height envelope, outflow, outflow decay, outflow mix, burner vertical term
+//   z       : swirl x term, burner cellular/lobe/radial z terms
+//   (y, z)  : turbulence x term     (x, z): turbulence y term, burner pulse
+//   (x, y)  : turbulence z term
+struct FxTabLayout {
+    int x, y, z, ltx, lty, ltz, pulse, total;
+};
+enum { TU_DECAY_Z = 0, TU_DECAY_W = 1, TU_TAMB4 = 2, TU_COUNT = 8 };
+enum { TX_SWZ = 0, TX_CELL = 1, TX_LOBE = 2, TX_RAD = 3, TX_COUNT = 4 };
+enum { TY_HE = 0, TY_OUT = 1, TY_DECAY = 2, TY_MIX = 3, TY_VERT = 4, TY_COUNT = 5 };
+enum { TZ_SWX = 0, TZ_CELL = 1, TZ_LOBE = 2, TZ_RAD = 3, TZ_COUNT = 4 };
+__host__ __device__ inline FxTabLayout fx_tab_layout(int X, int Y, int Z) {
+    FxTabLayout L;
+    L.x = TU_COUNT;
+    L.y = L.x + TX_COUNT * X;
+    L.z = L.y + TY_COUNT * Y;
+    L.ltx = L.z + TZ_COUNT * Z;
+    L.lty = L.ltx + Y * Z;
+    L.ltz = L.lty + X * Z;
+    L.pulse = L.ltz + X * Y;
+    L.total = L.pulse + X * Z;
+    return L;
+}
+
+// Burner geometry shared by the table entries (emitter, shaders.ts:101-133).
+struct FxBurnerGeom {
+    float time, cx, cz, radiusX, radiusZ, thickness;
+    float3 ext;
+};
+FXD FxBurnerGeom fx_burner_geom(const float* u) {
+    FxBurnerGeom G;
+    G.time = u[U_TIME];
+    G.ext = fx_extent(u);
+    G.cx = G.ext.x * 0.5f + sinf(G.time * FC(1.73)) * FC(0.013);
+    G.cz = G.ext.z * 0.5f + cosf(G.time * FC(1.37)) * FC(0.011);
     const float baseRadius = FC(0.1422673539502299);  // sqrt(0.02024), a WGSL const-expression
-    float radiusX = fx_min(baseRadius * fx_clamp(u[U_BURNER_X], FC(0.35), FC(3.2)), ext.x * FC(0.42));
-    float radiusZ = fx_min(baseRadius * fx_clamp(u[U_BURNER_Z], FC(0.35), FC(3.2)), ext.z * FC(0.42));
-    float thickness = fx_clamp(u[U_THICKNESS], FC(0.35), FC(2.5));
-    float radial = ox * ox / (radiusX * radiusX) + oz * oz / (radiusZ * radiusZ);
-    float vertical = oy * oy / (FC(0.0022) * thickness * thickness);
-    float cellular = FC(0.76) + FC(0.24) * sinf(px * 49.0f + time * FC(5.2)) * sinf(pz * 43.0f - time * FC(4.4));
-    float lobeArg = sinf(ox / fx_max(radiusX, FC(0.001)) * FC(6.2) + time * FC(1.7)) *
-                    sinf(oz / fx_max(radiusZ, FC(0.001)) * FC(5.4) - time * FC(1.3));
-    float lobes = fx_mix(FC(0.48), FC(1.18), fx_smoothstep(FC(-0.42), FC(0.48), lobeArg));
-    float texture = fx_mix(cellular, cellular * lobes, fx_clamp(u[U_CINEMATIC], 0.0f, 1.0f));
-    float pulse = FC(0.84) + FC(0.16) * sinf(time * FC(3.7) + px * 27.0f + pz * 21.0f);
-    return expf(-(radial + vertical)) * texture * pulse;
+    G.radiusX = fx_min(baseRadius * fx_clamp(u[U_BURNER_X], FC(0.35), FC(3.2)), G.ext.x * FC(0.42));
+    G.radiusZ = fx_min(baseRadius * fx_clamp(u[U_BURNER_Z], FC(0.35), FC(3.2)), G.ext.z * FC(0.42));
+    G.thickness = fx_clamp(u[U_THICKNESS], FC(0.35), FC(2.5));
+    return G;
+}
+
+// Table entry i of a simulation whose uniform block is u.
+FXD float fx_table_entry(const float* u, int X, int Y, int Z, int i) {
+    const FxTabLayout L = fx_tab_layout(X, Y, Z);
+    const float time = u[U_TIME], dt = u[U_DT];
+    const float persistence = fx_clamp(u[U_PERSISTENCE], FC(0.4), 3.0f);
+    auto nrm = [](int c, float dim) { return ((float)c + 0.5f) / dim; };
+    if (i < L.x) {
+        if (i == TU_DECAY_Z) return expf(-dt * FC(0.075) / persistence);
+        if (i == TU_DECAY_W) return expf(-dt * FC(0.14) / persistence);
+        if (i == TU_TAMB4) return powf(u[U_T_AMBIENT], 4.0f);
+        return 0.0f;
+    }
+    if (i < L.y) {
+        const int k = (i - L.x) / X, x = (i - L.x) - k * X;
+        const float nx = nrm(x, u[U_GRID_X]);
+        if (k == TX_SWZ) return cosf(u[U_TIME] * FC(1.9) + nx * 25.0f);
+        const FxBurnerGeom G = fx_burner_geom(u);
+        const float px = nx * G.ext.x, ox = px - G.cx;
+        if (k == TX_CELL) return sinf(px * 49.0f + time * FC(5.2));
+        if (k == TX_LOBE) return sinf(ox / fx_max(G.radiusX, FC(0.001)) * FC(6.2) + time * FC(1.7));
+        return ox * ox / (G.radiusX * G.radiusX);
+    }
+    if (i < L.z) {
+        const int k = (i - L.y) / Y, y = (i - L.y) - k * Y;
+        const float ny = nrm(y, u[U_GRID_Y]);
+        if (k == TY_HE) return fx_smoothstep(FC(0.045), FC(0.15), ny) * (1.0f - fx_smoothstep(FC(0.80), 1.0f, ny));
+        const float outflow = fx_smoothstep(FC(0.84), FC(0.995), ny);
+        if (k == TY_OUT) return outflow;
+        if (k == TY_DECAY) return expf(-outflow * dt * 15.0f / persistence);
+        if (k == TY_MIX) return outflow * FC(0.16) / persistence;
+        const FxBurnerGeom G = fx_burner_geom(u);
+        const float oy = ny * G.ext.y - FC(0.075);
+        return oy * oy / (FC(0.0022) * G.thickness * G.thickness);
+    }
+    if (i < L.ltx) {
+        const int k = (i - L.z) / Z, z = (i - L.z) - k * Z;
+        const float nz = nrm(z, u[U_GRID_Z]);
+        if (k == TZ_SWX) return sinf(u[U_TIME] * FC(2.3) + nz * 22.0f);
+        const FxBurnerGeom G = fx_burner_geom(u);
+        const float pz = nz * G.ext.z, oz = pz - G.cz;
+        if (k == TZ_CELL) return sinf(pz * 43.0f - time * FC(4.4));
+        if (k == TZ_LOBE) return sinf(oz / fx_max(G.radiusZ, FC(0.001)) * FC(5.4) - time * FC(1.3));
+        return oz * oz / (G.radiusZ * G.radiusZ);
+    }
+    if (i < L.lty) {  // turbulence x term, (y, z)
+        const int j = i - L.ltx, z = j / Y, y = j - z * Y;
+        const float ny = nrm(y, u[U_GRID_Y]), nz = nrm(z, u[U_GRID_Z]);
+        return sinf(ny * 31.0f + nz * 19.0f + time * FC(3.1)) + FC(0.45) * sinf(ny * 67.0f - time * FC(5.3));
+    }
+    if (i < L.ltz) {  // turbulence y term, (x, z)
+        const int j = i - L.lty, z = j / X, x = j - z * X;
+        const float nx = nrm(x, u[U_GRID_X]), nz = nrm(z, u[U_GRID_Z]);
+        return FC(0.12) * sinf(nx * 29.0f + nz * 23.0f - time * FC(4.1));
+    }
+    if (i < L.pulse) {  // turbulence z term, (x, y)
+        const int j = i - L.ltz, y = j / X, x = j - y * X;
+        const float nx = nrm(x, u[U_GRID_X]), ny = nrm(y, u[U_GRID_Y]);
+        return cosf(ny * 27.0f - nx * 21.0f + time * FC(2.7)) + FC(0.45) * cosf(ny * 59.0f + time * FC(4.7));
+    }
+    {  // burner pulse, (x, z)
+        const int j = i - L.pulse, z = j / X, x = j - z * X;
+        const FxBurnerGeom G = fx_burner_geom(u);
+        const float px = nrm(x, u[U_GRID_X]) * G.ext.x, pz = nrm(z, u[U_GRID_Z]) * G.ext.z;
+        return FC(0.84) + FC(0.16) * sinf(time * FC(3.7) + px * 27.0f + pz * 21.0f);
+    }
 }
 
 struct FxCellOut {
@@ -64,12 +206,13 @@ struct FxCellOut {
 // boundary ambient, liquid cooling, entrainment, Arrhenius burn, vorticity confinement,
 // turbulence, buoyancy, spray momentum, radiation, open-top outflow and wall clamps.
 template <class Acc>
-FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y, int z, const Acc& a) {
+FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y, int z, const Acc& a,
+                               const float* __restrict__ tab, const FxDivc* __restrict__ dc) {
     const float* u = P.u;
     const int X = g.X, Y = g.Y, Z = g.Z;
-    long long id = g.idx(x, y, z);
+    const FxTabLayout L = fx_tab_layout(X, Y, Z);
+    const int id = x + X * (y + Y * z);
     float picx = (float)x + 0.5f, picy = (float)y + 0.5f, picz = (float)z + 0.5f;
-    float nx = picx / u[U_GRID_X], ny = picy / u[U_GRID_Y], nz = picz / u[U_GRID_Z];
     float dt = u[U_DT];
 
     float4 orig = a.flow(id);
@@ -77,32 +220,39 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     float btx = picx - orig.x * dt * metric.x;
     float bty = picy - orig.y * dt * metric.y;
     float btz = picz - orig.z * dt * metric.z;
-    float4 flow = fx_trilinear(g, u, btx, bty, btz, [&](long long i) { return a.flow(i); });
-    float4 species = fx_trilinear(g, u, btx, bty, btz, [&](long long i) { return a.species(i); });
+    const FxTri tri = fx_tri_setup(g, u, btx, bty, btz);
+    float4 flow = fx_trilinear(g, tri, [&](int i) { return a.flow(i); });
+    float4 species = fx_trilinear(g, tri, [&](int i) { return a.species(i); });
     species = make_float4(fx_max(species.x, 0.0f), fx_max(species.y, 0.0f), fx_max(species.z, 0.0f),
                           fx_max(species.w, 0.0f));
 
-    float4 left = a.flow(g.idx(x - 1, y, z)), right = a.flow(g.idx(x + 1, y, z));
-    float4 bottom = a.flow(g.idx(x, y - 1, z)), top = a.flow(g.idx(x, y + 1, z));
-    float4 back = a.flow(g.idx(x, y, z - 1)), front = a.flow(g.idx(x, y, z + 1));
+    // 6 neighbours with clamped (Neumann) addressing (shaders.ts:43-51)
+    const int oL = x > 0 ? id - 1 : id, oR = x < X - 1 ? id + 1 : id;
+    const int oB = y > 0 ? id - X : id, oT = y < Y - 1 ? id + X : id;
+    const int oK = z > 0 ? id - X * Y : id, oF = z < Z - 1 ? id + X * Y : id;
+    float4 left = a.flow(oL), right = a.flow(oR);
+    float4 bottom = a.flow(oB), top = a.flow(oT);
+    float4 back = a.flow(oK), front = a.flow(oF);
 
     {  // 6-neighbour diffusion of velocity and temperature (shaders.ts:177-180)
-        float vax = (left.x + right.x + bottom.x + top.x + back.x + front.x) / 6.0f;
-        float vay = (left.y + right.y + bottom.y + top.y + back.y + front.y) / 6.0f;
-        float vaz = (left.z + right.z + bottom.z + top.z + back.z + front.z) / 6.0f;
+        float vax = fx_divc(left.x + right.x + bottom.x + top.x + back.x + front.x, dc[DIVC_SIX]);
+        float vay = fx_divc(left.y + right.y + bottom.y + top.y + back.y + front.y, dc[DIVC_SIX]);
+        float vaz = fx_divc(left.z + right.z + bottom.z + top.z + back.z + front.z, dc[DIVC_SIX]);
         float vm = fx_clamp(dt * FC(0.32), 0.0f, FC(0.12));
         flow.x = fx_mix(flow.x, vax, vm);
         flow.y = fx_mix(flow.y, vay, vm);
         flow.z = fx_mix(flow.z, vaz, vm);
-        float ta = (left.w + right.w + bottom.w + top.w + back.w + front.w) / 6.0f;
+        float ta = fx_divc(left.w + right.w + bottom.w + top.w + back.w + front.w, dc[DIVC_SIX]);
         flow.w = fx_mix(flow.w, ta, fx_clamp(dt * FC(0.18), 0.0f, FC(0.08)));
     }
     {  // species diffusion (shaders.ts:182-187)
-        float4 sl = a.species(g.idx(x - 1, y, z)), sr = a.species(g.idx(x + 1, y, z));
-        float4 sb = a.species(g.idx(x, y - 1, z)), st = a.species(g.idx(x, y + 1, z));
-        float4 sk = a.species(g.idx(x, y, z - 1)), sf = a.species(g.idx(x, y, z + 1));
-        float4 avg = make_float4((sl.x + sr.x + sb.x + st.x + sk.x + sf.x) / 6.0f, (sl.y + sr.y + sb.y + st.y + sk.y + sf.y) / 6.0f,
-                                 (sl.z + sr.z + sb.z + st.z + sk.z + sf.z) / 6.0f, (sl.w + sr.w + sb.w + st.w + sk.w + sf.w) / 6.0f);
+        float4 sl = a.species(oL), sr = a.species(oR);
+        float4 sb = a.species(oB), st = a.species(oT);
+        float4 sk = a.species(oK), sf = a.species(oF);
+        float4 avg = make_float4(fx_divc(sl.x + sr.x + sb.x + st.x + sk.x + sf.x, dc[DIVC_SIX]),
+                                 fx_divc(sl.y + sr.y + sb.y + st.y + sk.y + sf.y, dc[DIVC_SIX]),
+                                 fx_divc(sl.z + sr.z + sb.z + st.z + sk.z + sf.z, dc[DIVC_SIX]),
+                                 fx_divc(sl.w + sr.w + sb.w + st.w + sk.w + sf.w, dc[DIVC_SIX]));
         species = fx_mix4(species, avg, fx_clamp(dt * FC(0.12), 0.0f, FC(0.06)));
     }
 
@@ -121,15 +271,22 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
             species.x = fx_max(species.x, sp.fuel * j);
             flow.w = fx_max(flow.w, u[U_T_AMBIENT] + (sp.temperature - u[U_T_AMBIENT]) * j);
         }
-    } else {
-        source = fx_burner(u, nx, ny, nz);
+    } else {  // emitter (shaders.ts:101-133) from the per-step tables
+        const float radial = __ldg(tab + L.x + TX_RAD * X + x) + __ldg(tab + L.z + TZ_RAD * Z + z);
+        const float vertical = __ldg(tab + L.y + TY_VERT * Y + y);
+        const float cellular = FC(0.76) + FC(0.24) * __ldg(tab + L.x + TX_CELL * X + x) * __ldg(tab + L.z + TZ_CELL * Z + z);
+        const float lobeArg = __ldg(tab + L.x + TX_LOBE * X + x) * __ldg(tab + L.z + TZ_LOBE * Z + z);
+        const float lobes = fx_mix(FC(0.48), FC(1.18), fx_smoothstep_c(FC(-0.42), lobeArg, dc[DIVC_LOBE]));
+        const float texture = fx_mix(cellular, cellular * lobes, fx_clamp(u[U_CINEMATIC], 0.0f, 1.0f));
+        const float pulse = __ldg(tab + L.pulse + z * X + x);
+        source = expf(-(radial + vertical)) * texture * pulse;
         species.x = fx_max(species.x, source * u[U_FUEL_RATE] * firePower);
         flow.w = fx_max(flow.w, u[U_T_AMBIENT] + source * 1180.0f * thermalPower);
     }
     {
-        float swx = sinf(u[U_TIME] * FC(2.3) + nz * 22.0f);
+        float swx = __ldg(tab + L.z + TZ_SWX * Z + z);
         float swy = 0.0f;
-        float swz = cosf(u[U_TIME] * FC(1.9) + nx * 25.0f);
+        float swz = __ldg(tab + L.x + TX_SWZ * X + x);
         float s = source * dt * FC(0.11) * u[U_VORTICITY] * powerRoot;
         flow.x = flow.x + swx * s;
         flow.y = flow.y + swy * s;
@@ -142,21 +299,28 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         flow.w = fx_mix(flow.w, u[U_T_AMBIENT], FC(0.035));
     }
 
-    // Liquid cooling and vapor (shaders.ts:212-215)
-    float water = fx_clamp((float)a.liquid(id) * (1.0f / 4096.0f) * FC(3.4), 0.0f, 5.0f);
-    float evaporation = water * fx_smoothstep(335.0f, 1040.0f, flow.w) * dt * FC(13.5);
-    flow.w = fx_max(u[U_T_AMBIENT], flow.w - evaporation * 2080.0f - water * dt * 260.0f);
-    species.w = fx_clamp(species.w + evaporation * FC(2.15), 0.0f, 3.0f);
+    // Liquid cooling and vapor (shaders.ts:212-215). With no liquid (water == +0) every
+    // product below is +0 and the updates reduce exactly to max/clamp of the inputs.
+    const uint32_t liquidRaw = a.liquid(id);
+    float water = fx_clamp((float)liquidRaw * (1.0f / 4096.0f) * FC(3.4), 0.0f, 5.0f);
+    if (liquidRaw) {
+        float evaporation = water * fx_smoothstep_c(335.0f, flow.w, dc[DIVC_EVAP]) * dt * FC(13.5);
+        flow.w = fx_max(u[U_T_AMBIENT], flow.w - evaporation * 2080.0f - water * dt * 260.0f);
+        species.w = fx_clamp(species.w + evaporation * FC(2.15), 0.0f, 3.0f);
+    } else {
+        flow.w = fx_max(u[U_T_AMBIENT], flow.w);             // x - (+0) == x exactly
+        species.w = fx_clamp(species.w + 0.0f, 0.0f, 3.0f);  // x + (+0) maps -0 to +0, as the full form
+    }
 
     // O2 entrainment (shaders.ts:220-232)
     float entrainment = fx_clamp(u[U_ENTRAIN], 0.0f, 3.0f);
     float ambientOxygen = fx_max(u[U_OXYGEN], FC(0.001));
-    float oxygenDeficit = fx_clamp((ambientOxygen - species.y) / ambientOxygen, 0.0f, 1.0f);
-    float fuelCore = fx_smoothstep(FC(0.30), FC(0.78), species.x);
+    float oxygenDeficit = fx_clamp(fx_divc(ambientOxygen - species.y, dc[DIVC_AMBIENT_O2]), 0.0f, 1.0f);
+    float fuelCore = fx_smoothstep_c(FC(0.30), species.x, dc[DIVC_FUELCORE]);
     float interfaceWeight = oxygenDeficit * fx_mix(1.0f, FC(0.18), fuelCore);
     float entrainmentMix = fx_clamp(dt * entrainment *
                                         (FC(0.12) + FC(0.28) * fx_length3(flow.x, flow.y, flow.z) +
-                                         FC(0.22) * fx_smoothstep(400.0f, 1500.0f, flow.w)) *
+                                         FC(0.22) * fx_smoothstep_c(400.0f, flow.w, dc[DIVC_ENTRAIN_T])) *
                                         interfaceWeight,
                                     0.0f, FC(0.08));
     species.y = fx_mix(species.y, ambientOxygen, entrainmentMix);
@@ -165,12 +329,21 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     float fuelBefore = fx_max(species.x, 0.0f);
     float oxygenBefore = fx_max(species.y, 0.0f);
     float availableFuel = fx_min(fuelBefore, oxygenBefore * FC(0.25));
-    float safeFuel = fx_max(fuelBefore, FC(0.00001));
-    float safeOxygen = fx_max(oxygenBefore, FC(0.00001));
-    float activation = expf(-15000.0f / fx_max(flow.w, u[U_T_AMBIENT]));
-    float arrhenius = fx_clamp(FC(2.5e6) * activation * powf(safeFuel, FC(-0.30)) * powf(safeOxygen, FC(1.30)), 0.0f, 80.0f);
-    float ignition = fx_smoothstep(690.0f, 930.0f, flow.w);
-    float requestedBurn = availableFuel * (1.0f - expf(-arrhenius * ignition * dt)) * expf(-water * 18.0f);
+    float ignition = fx_smoothstep_c(690.0f, flow.w, dc[DIVC_IGNITION]);
+    // 1 - exp(-arrhenius * ignition * dt). Below ignition (ignition == +0) the exponent is
+    // -0 for any finite rate (the rate is clamped to [0, 80]) and the factor is exactly
+    // +0, so the rate need not be evaluated; with no liquid exp(-water * 18) is exactly 1.
+    float growth = 0.0f;
+    if (!(ignition == 0.0f)) {
+        float safeFuel = fx_max(fuelBefore, FC(0.00001));
+        float safeOxygen = fx_max(oxygenBefore, FC(0.00001));
+        float activation = expf(-15000.0f / fx_max(flow.w, u[U_T_AMBIENT]));
+        float arrhenius =
+            fx_clamp(FC(2.5e6) * activation * powf(safeFuel, FC(-0.30)) * powf(safeOxygen, FC(1.30)), 0.0f, 80.0f);
+        growth = 1.0f - expf(-arrhenius * ignition * dt);
+    }
+    float requestedBurn = availableFuel * growth;
+    if (liquidRaw) requestedBurn = requestedBurn * expf(-water * 18.0f);
     float burn = fx_clamp(requestedBurn, 0.0f, availableFuel);
     float richness = fx_clamp(1.0f - oxygenBefore / fx_max(fuelBefore * 4.0f, FC(0.00001)), 0.0f, 1.0f);
     species.x = fx_max(0.0f, fuelBefore - burn);
@@ -178,7 +351,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     species.z = fx_clamp(species.z + burn * (1.0f + richness * FC(1.8)), 0.0f, 3.0f);
     species.w = fx_clamp(species.w + burn * FC(0.62), 0.0f, 3.0f);
     flow.w += burn * (2150.0f + 1450.0f * u[U_HEAT_EFF]);
-    float reaction = fx_clamp(burn / fx_max(dt, FC(0.0001)) * FC(0.22), 0.0f, 4.0f);
+    float reaction = fx_clamp(fx_divc(burn, dc[DIVC_DT]) * FC(0.22), 0.0f, 4.0f);
 
     {  // vorticity confinement: curl x grad(T) (shaders.ts:258-272)
         float cx = 0.5f * ((top.z - bottom.z) * metric.y - (front.y - back.y) * metric.z);
@@ -197,22 +370,21 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         flow.z = flow.z + (gx * cy - gy * cx) * vs;
     }
     {  // height-enveloped turbulence (shaders.ts:274-285)
-        float time = u[U_TIME];
-        float hotPlume = fx_smoothstep(520.0f, 1650.0f, flow.w);
-        float heightEnvelope = fx_smoothstep(FC(0.045), FC(0.15), ny) * (1.0f - fx_smoothstep(FC(0.80), 1.0f, ny));
-        float ltx = sinf(ny * 31.0f + nz * 19.0f + time * FC(3.1)) + FC(0.45) * sinf(ny * 67.0f - time * FC(5.3));
-        float lty = FC(0.12) * sinf(nx * 29.0f + nz * 23.0f - time * FC(4.1));
-        float ltz = cosf(ny * 27.0f - nx * 21.0f + time * FC(2.7)) + FC(0.45) * cosf(ny * 59.0f + time * FC(4.7));
+        float hotPlume = fx_smoothstep_c(520.0f, flow.w, dc[DIVC_HOTPLUME]);
+        float heightEnvelope = __ldg(tab + L.y + TY_HE * Y + y);
+        float ltx = __ldg(tab + L.ltx + z * Y + y);
+        float lty = __ldg(tab + L.lty + z * X + x);
+        float ltz = __ldg(tab + L.ltz + y * X + x);
         float ts = (FC(0.075) + FC(0.16) * u[U_VORTICITY]) * hotPlume * heightEnvelope * dt;
         flow.x = flow.x + ltx * ts;
         flow.y = flow.y + lty * ts;
         flow.z = flow.z + ltz * ts;
     }
     {  // buoyancy (shaders.ts:287-288)
-        float buoyancy = fx_clamp((flow.w - u[U_T_AMBIENT]) / 1500.0f, FC(-0.1), FC(1.2));
+        float buoyancy = fx_clamp(fx_divc(flow.w - u[U_T_AMBIENT], dc[DIVC_BUOYANCY]), FC(-0.1), FC(1.2));
         flow.y += buoyancy * dt * FC(0.72) * fx_clamp(u[U_BUOYANCY], 0.0f, 4.0f);
     }
-    species.z *= expf(-water * dt * FC(4.8));
+    if (liquidRaw) species.z *= expf(-water * dt * FC(4.8));  // exp(-0) == 1 exactly otherwise
     {  // spray momentum (shaders.ts:293-297)
         float3 ext = fx_extent(u);
         float ox = FC(0.035) * ext.x, oy = FC(0.50) * ext.y, oz = FC(0.5) * ext.z;
@@ -228,18 +400,18 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     }
     // radiation and decay (shaders.ts:299-304)
     float persistence = fx_clamp(u[U_PERSISTENCE], FC(0.4), 3.0f);
-    float radiation = FC(5.67e-8) * (powf(u[U_T_AMBIENT], 4.0f) - powf(fx_max(flow.w, 0.0f), 4.0f)) / (1005.0f * persistence);
+    float radiation = fx_divc(FC(5.67e-8) * (__ldg(tab + TU_TAMB4) - powf(fx_max(flow.w, 0.0f), 4.0f)), dc[DIVC_RADIATION]);
     flow.w = fx_max(u[U_T_AMBIENT], flow.w + dt * radiation);
-    species.z *= expf(-dt * FC(0.075) / persistence);
-    species.w *= expf(-dt * FC(0.14) / persistence);
+    species.z *= __ldg(tab + TU_DECAY_Z);
+    species.w *= __ldg(tab + TU_DECAY_W);
 
     // open-top outflow (shaders.ts:308-321)
-    float outflow = fx_smoothstep(FC(0.84), FC(0.995), ny);
+    float outflow = __ldg(tab + L.y + TY_OUT * Y + y);
     species.x *= 1.0f - outflow;
-    float outflowDecay = expf(-outflow * dt * 15.0f / persistence);
+    float outflowDecay = __ldg(tab + L.y + TY_DECAY * Y + y);
     species.z *= outflowDecay;
     species.w *= outflowDecay;
-    flow.w = fx_mix(flow.w, u[U_T_AMBIENT], outflow * FC(0.16) / persistence);
+    flow.w = fx_mix(flow.w, u[U_T_AMBIENT], __ldg(tab + L.y + TY_MIX * Y + y));
     reaction *= 1.0f - outflow;
     if (y == Y - 1) {
         species.x = 0.0f;
@@ -291,21 +463,3 @@ FXD float fx_jacobi_update(const FxJacobiConst& c, float l, float r, float b, fl
     return __fdiv_rn(fx_jacobi_numerator(c, l, r, b, t, k, f, div), c.denom);
 }
 
-// Division by a constant d > 0 given rcp = RN(1/d): Markstein's correction step
-// (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Dev. 34(1), 1990): q = RN(x*rcp), e = x - q*d exactly by one
-// fused multiply-add, result RN(q + e*rcp). The theorem assumes no underflow, so the
-// step is used for 2^-96 <= |x| <= FLT_MAX (the quotient stays normal for any d below
-// 2^30); zeros (whose sign must survive) and tiny x take the IEEE division, and
-// x = +-inf or NaN, whose IEEE quotient by a finite d > 0 is x itself, is returned. The
-// engine enables this path for a given d only after checking on the device that it
-// equals IEEE x/d for every float x.
-FXD float fx_div_by_const(float x, float d, float rcp) {
-    const float ax = fabsf(x);
-    if (ax >= 1.2621774483536189e-29f && ax <= 3.402823466e38f) {  // 2^-96 .. FLT_MAX
-        const float q = __fmul_rn(x, rcp);
-        const float e = __fmaf_rn(-q, d, x);
-        return __fmaf_rn(e, rcp, q);
-    }
-    return ax <= 3.402823466e38f ? __fdiv_rn(x, d) : x;
-}
