@@ -18,6 +18,8 @@ ERR_TIMEOUT = -5
 ERR_UNSUPPORTED = -6
 ERR_STATE = -7
 
+NOALLOC_MAX_PLANES = 2048  # interior z planes the no-allocation norm's static scratch holds
+
 PRECISION_F32 = 0
 PRECISION_MIXED = 1
 
@@ -148,6 +150,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_read_field": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_write_field": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_divergence_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
+        "firex_divergence_norm_noalloc": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float), vp,
+                                                    C.POINTER(C.c_double)]),
         "firex_get_state": (C.c_int, [vp, C.POINTER(State)]),
         "firex_set_state": (C.c_int, [vp, C.POINTER(State)]),
         "firex_get_uniforms": (C.c_int, [vp, C.c_double, C.POINTER(C.c_float)]),
@@ -182,7 +186,8 @@ def declare_firex(lib: C.CDLL) -> None:
 HEADER_SYMBOLS = [
     "firex_default_options", "firex_field_element_size", "firex_create", "firex_destroy",
     "firex_last_error", "firex_set_parameter", "firex_get_parameter", "firex_reset", "firex_step",
-    "firex_sync", "firex_read_field", "firex_write_field", "firex_divergence_norm", "firex_get_state",
+    "firex_sync", "firex_read_field", "firex_write_field", "firex_divergence_norm",
+    "firex_divergence_norm_noalloc", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_stream", "firex_set_profiling", "firex_pass_times",
     "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_batch_create", "firex_batch_destroy",

@@ -190,6 +190,10 @@ int zm_chunk(long long tiles32, long long tiles16) {
 
 }  // namespace
 
+// Sets the text that firex_last_error(NULL) returns on this thread (entry points that
+// have no handle report through it).
+void fx_set_thread_error(const std::string& msg) { g_create_error = msg; }
+
 struct firex_batch;
 
 // Whether fx_div_by_const(x, d, rcp) equals IEEE x / d for every finite float x on this

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 
 #include "fx_device.cuh"
 
@@ -35,3 +36,6 @@ void fx_launch_upload_batch(cudaStream_t s, const FxBatchDev& host, FxBatchDev* 
 
 // Exhaustive check of fx_div_by_const against IEEE division for one denominator.
 void fx_launch_check_div(cudaStream_t s, float d, float rcp, float lo, float hi, unsigned long long* mismatches);
+
+// Sets the text that firex_last_error(NULL) returns on the calling thread (fx_engine.cu).
+void fx_set_thread_error(const std::string& msg);

@@ -131,7 +131,8 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
 /* Releases every device allocation. Replaces FireXEngine.dispose (FireXEngine.ts:1034). */
 int firex_destroy(firex_sim* sim);
 
-/* Text of the last failure on sim (or of the last failed firex_create when sim is NULL). */
+/* Text of the last failure on sim (or, when sim is NULL, of the last failed firex_create
+ * or firex_divergence_norm_noalloc on the calling thread). */
 const char* firex_last_error(const firex_sim* sim);
 
 /* Named engine parameter with the reference's clamps and fallbacks
@@ -166,6 +167,27 @@ int firex_write_field(firex_sim* sim, int32_t field, const void* host, size_t by
  * excluded, qualityShaders.ts:47-57), reduced in FP64: out[0] = L2 norm, out[1] = max
  * abs, out[2] = number of interior cells. (Presentation diagnostic, FireXEngine.ts:2588-2596.) */
 int firex_divergence_norm(firex_sim* sim, double out[3]);
+
+/* The same norm for a flow field the caller owns, with no device allocation: for hosts
+ * whose device memory belongs to their own pool or budget, or whose frame or serving loop
+ * must not stall on cudaMalloc/cudaFree (both may synchronise the device), and which
+ * therefore cannot let the library allocate or create a handle just for a norm.
+ * No counterpart in the reference (its divergence view is a presentation pass).
+ *
+ * flow: device pointer, 16-byte aligned, dims[0]*dims[1]*dims[2] float4 records (u v w T)
+ * with cell index x + X*(y + Y*z) (the layout of FIREX_FIELD_FLOW); metric: grid/domain
+ * per axis as FP32 (shaders.ts:39-41); stream: cudaStream_t as void* (NULL: the legacy
+ * default stream) on the device that owns flow. out[0] = L2, out[1] = max abs, out[2] =
+ * interior cell count, as firex_divergence_norm. Returns after the result reached out.
+ *
+ * Scratch is a 32 KiB array in the library's device image (held on every GPU that loads
+ * the library until exit), one slot pair per interior z plane: Z - 2 above
+ * FIREX_NOALLOC_MAX_PLANES is rejected with FIREX_ERR_BAD_ARG. The first call on a device
+ * looks up that array's device address; make it before any stream capture. Calls share
+ * the array, so calls that overlap on a GPU race: serialise them. */
+#define FIREX_NOALLOC_MAX_PLANES 2048
+int firex_divergence_norm_noalloc(const void* flow, const int32_t dims[3], const float metric[3], void* stream,
+                                  double out[3]);
 
 /* Counters that decide ping-pong parity and time (FireXEngine.ts:396-409). */
 int firex_get_state(const firex_sim* sim, firex_state* st);
