@@ -47,6 +47,17 @@ JACOBI_BYTES_PER_CELL = 12  # read p + read div + write p, f32 (algorithmic, per
 L2_BYTES = 126 * 1024 * 1024
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the default
+# Jacobi kernel on this workload, from one ncu capture (profiles/jacobi_unblocked_hd.md).
+JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768}
+
+
+def jacobi_kernel_name(diag: dict) -> str:
+    if diag.get("jacobi_block", 1) > 1:
+        return "fxk_jacobi_tb<K=%d>" % diag["jacobi_block"]
+    return "fxk_jacobi_zm<float>" if diag.get("jacobi_zchunk", 0) > 0 else "fxk_jacobi<float>"
+
+
 def cells() -> int:
     return DIMS[0] * DIMS[1] * DIMS[2]
 
@@ -234,7 +245,8 @@ def run_gpu(args) -> None:
     barrier()
     step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     total_ms = evs[0].elapsed_time(evs[-1])
-    launches = sum(n for _, n in sim.pass_times().values())
+    diag = sim.diagnostics
+    launches = diag["launches_per_step"] * args.steps  # kernel nodes of the replayed step graph
     total_ms_max = max_over_ranks(total_ms)
     value = n_cells * args.steps * world / (total_ms_max / 1e3) / 1e9
 
@@ -269,13 +281,8 @@ def run_gpu(args) -> None:
     jac_avg_ms = jac_ms / max(1, jac_n)
     peak, peak_kind = measured_peak_hbm()
     achieved = JACOBI_BYTES_PER_CELL * n_cells / (jac_avg_ms / 1e3) / 1e9
-    traffic = None
-    tp = ROOT / "profiles" / "jacobi_f32_traffic.json"
-    if tp.exists():
-        try:
-            traffic = json.loads(tp.read_text()).get("bytes_per_launch_hd")
-        except Exception:
-            traffic = None
+    kernel = jacobi_kernel_name(diag)
+    traffic = JACOBI_TRAFFIC_PER_LAUNCH.get(kernel)
 
     if rank == 0:
         cpu = None
@@ -290,7 +297,7 @@ def run_gpu(args) -> None:
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 384,
                     "d2h_bytes_per_step": n_cells * 16, "steps": e2e_steps,
                     "what": "firex_step (384 B parameter block host->device) + firex_read_field(FLOW) into pinned host memory, every step"},
-            "roofline": {"kernel": "fxk_jacobi_f32", "bound": "hbm", "achieved": achieved, "peak": peak,
+            "roofline": {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "traffic": traffic, "bytes_per_cell": JACOBI_BYTES_PER_CELL, "avg_launch_us": jac_avg_ms * 1e3,
                          "launches": jac_n},
