@@ -49,6 +49,7 @@ JACOBI_AUTO = 0
 JACOBI_UNBLOCKED = 1
 JACOBI_ZMARCH = 2
 JACOBI_FUSED = 3
+JACOBI_RESIDENT = 4
 
 VALUE_NUMBER = 0
 VALUE_BOOLEAN = 1
@@ -117,7 +118,8 @@ class Diagnostics(C.Structure):
         ("jacobi_zchunk", C.c_int32),
         ("graph", C.c_int32),
         ("launches_per_step", C.c_int32),
-        ("reserved", C.c_int32 * 11),
+        ("jacobi_kernel", C.c_int32),
+        ("reserved", C.c_int32 * 10),
     ]
 
 

@@ -163,13 +163,30 @@ struct __align__(16) FxSimDev {
     uint32_t* liquid;
     float* tab;            // per-step tables of simulate (fx_step_math.cuh)
     FxDivc divc[DIVC_COUNT];
+    unsigned* sync;        // [2]: error word (a bounded device wait expired); from
+                           // FX_RES_FLAGS: the resident Jacobi's per-box flags of both
+                           // phases (zeroed at every step start)
 };
 
 // Work decomposition shared by every batched pass: each pass walks a flat list of
 // bricks across all simulations of a batch; start[shape][s] is the first brick of
 // simulation s (prefix sums over the batch), so one launch covers uneven grids.
 #define FX_MAX_BATCH 512
-enum FxShape { FX_SHAPE_CELL = 0, FX_SHAPE_ROW4 = 1, FX_SHAPE_COL = 2, FX_SHAPE_ZM = 3, FX_SHAPE_TAB = 4, FX_NSHAPES = 5 };
+enum FxShape {
+    FX_SHAPE_CELL = 0,
+    FX_SHAPE_ROW4 = 1,
+    FX_SHAPE_COL = 2,
+    FX_SHAPE_ZM = 3,
+    FX_SHAPE_TAB = 4,
+    FX_SHAPE_RES = 5,  // one CTA per box of the resident Jacobi (fx_jacobi_res.cuh)
+    FX_NSHAPES = 6
+};
+
+// Box decomposition of one simulation for the resident Jacobi: boxes of by x bz rows of
+// full x rows, nby x nbz of them (CTA b owns box (b % nby, b / nby)).
+struct FxResBox {
+    int by, bz, nby, nbz;
+};
 // CELL: 32 x 4 x 2 cells, one thread per cell (simulate).
 // ROW4: 256 groups of 4 consecutive x cells in memory order (stencils).
 // COL : column tiles of the temporally blocked Jacobi (see fx_jacobi_tb.cuh).
@@ -187,7 +204,32 @@ struct FxBatchDev {
     int colTileX, colTileY;        // interior tile of the COL shape
     FxSimDev* sims[FX_MAX_BATCH];
     int start[FX_NSHAPES][FX_MAX_BATCH + 1];
+    FxResBox res[FX_MAX_BATCH];
 };
+
+// Buffers of launch `launch` of a solve phase: launches alternate between the two
+// buffers of the phase starting from the warm-start parity (primary, branches A and B)
+// or from buffer 0 (residual, and the cold primary of branch C); the first launch of a
+// cleared solve has a zero input.
+struct FxSolveBufs {
+    const void* pin;
+    void* pout;
+    bool zeroIn;
+};
+FXD FxSolveBufs fx_solve_bufs(const FxSimDev& S, int phase, int launch) {
+    FxSolveBufs r;
+    if (phase == 0) {
+        const int base = (S.mode == FIREX_PRESSURE_COLD_F32) ? 0 : S.pi;
+        r.pin = S.p[(base + launch) & 1];
+        r.pout = S.p[(base + launch + 1) & 1];
+        r.zeroIn = S.mode == FIREX_PRESSURE_COLD_F32 && launch == 0;
+    } else {
+        r.pin = S.corr[launch & 1];
+        r.pout = S.corr[(launch + 1) & 1];
+        r.zeroIn = launch == 0;
+    }
+    return r;
+}
 
 // Finds the simulation owning brick w (start[] ascending, start[nsims] = total).
 FXD int fx_find_sim(const int* __restrict__ start, int nsims, int w) {

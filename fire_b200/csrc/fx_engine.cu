@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdlib>
 #include <cmath>
 #include <cstdio>
@@ -22,6 +23,7 @@
 
 #include "../../include/firex.h"
 #include "fx_internal.h"
+#include "fx_jacobi_res.cuh"
 #include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
 
@@ -127,10 +129,12 @@ struct StepPlan {
     int zmZc = 16;            // z planes per CTA of the single-sweep (z-marching) kernel
     bool row4 = false;        // single sweeps by the unblocked kernel instead
     bool fuseP = false, fuseR = false;
-    int bricks[FX_NSHAPES] = {0, 0, 0, 0, 0};
+    bool res = false;         // every sweep of a phase in one resident launch
+    int resSmem = 0;          // its dynamic shared memory per CTA
+    int bricks[FX_NSHAPES] = {};
     auto key() const {
-        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, bricks[0], bricks[1], bricks[2],
-                        bricks[3], bricks[4]);
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, res, resSmem, bricks[0],
+                        bricks[1], bricks[2], bricks[3], bricks[4], bricks[5]);
     }
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
 };
@@ -142,12 +146,17 @@ bool can_fuse(int k, int n) { return k > 1 && n >= k && ((k - 1) * (n / k)) % 2 
 
 int jacobi_phase_launches(const StepPlan& pl, int phase) {
     const int n = phase == 0 ? pl.maxP : pl.maxR;
+    if (pl.res) return n > 0 ? 1 : 0;
     const bool fuse = phase == 0 ? pl.fuseP : pl.fuseR;
     return fuse ? n / pl.k + n % pl.k : n;
 }
 
 void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, int phase) {
     const int n = phase == 0 ? pl.maxP : pl.maxR;
+    if (pl.res) {  // a failed launch is reported by the caller's cudaGetLastError
+        if (n > 0) fx_launch_jacobi_res(st, pl.half, B, pl.bricks[FX_SHAPE_RES], phase, pl.resSmem);
+        return;
+    }
     const bool fuse = phase == 0 ? pl.fuseP : pl.fuseR;
     int launch = 0, sweep = 0;
     if (fuse) {
@@ -180,6 +189,81 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
 void default_jacobi(long long cells, int* kernel, int* zc) {
     *kernel = cells >= (16LL << 20) ? FIREX_JACOBI_ZMARCH : FIREX_JACOBI_UNBLOCKED;
     *zc = 32;
+}
+
+// Box decomposition of an X x Y x Z grid over at most m CTAs for the resident Jacobi.
+// A CTA's threads take the box's (x group, row) columns, each split into parts along z
+// when columns are fewer than threads, so a thread computes zlen = ceil(bz / parts)
+// groups per sweep. Cost per sweep: zlen plus the halo traffic per thread (faces written
+// and halo rows read, 2 (by + bz) rows of X / 4 groups, both ways). False when no box
+// fits one CTA's shared memory and registers.
+bool res_box(int X, int Y, int Z, int m, FxResBox* out) {
+    const int gx = X / 4;
+    bool found = false;
+    double best = 0;
+    for (int by = 1; by <= Y && (long long)by * gx <= FX_RES_THREADS; ++by) {
+        const int nby = (Y + by - 1) / by;
+        if (nby > m || nby > FX_RES_MAX_CTAS) continue;
+        const int maxNbz = m / nby;
+        const int bz = (Z + maxNbz - 1) / maxNbz;
+        if (fx_res_smem_bytes(X, by, bz) > FX_RES_SMEM_MAX) continue;
+        const int parts = FX_RES_THREADS / (by * gx);
+        const int zlen = (bz + parts - 1) / parts;
+        if (zlen > FX_RES_MAXG) continue;
+        const double cost = zlen + 4.0 * (by + bz) * gx / FX_RES_THREADS;
+        if (!found || cost < best) {
+            found = true;
+            best = cost;
+            *out = FxResBox{by, bz, nby, (Z + bz - 1) / bz};
+        }
+    }
+    return found;
+}
+
+// CTAs for every simulation of a batch within `cap` (one launch): each gets at least the
+// fewest CTAs its grid fits in, the rest in proportion to cells. False when the batch
+// does not fit.
+bool res_assign(const std::vector<std::array<int, 3>>& dims, int cap, std::vector<FxResBox>* boxes, int* smem) {
+    const size_t n = dims.size();
+    if (n == 0 || cap <= 0) return false;
+    std::vector<int> mins(n), t(n);
+    long long sumMin = 0;
+    double cells = 0;
+    FxResBox tmp;
+    for (size_t i = 0; i < n; ++i) {
+        const auto& d = dims[i];
+        if (!res_box(d[0], d[1], d[2], cap, &tmp)) return false;
+        int lo = 1, hi = cap;
+        while (lo < hi) {
+            const int mid = (lo + hi) / 2;
+            if (res_box(d[0], d[1], d[2], mid, &tmp)) hi = mid;
+            else lo = mid + 1;
+        }
+        mins[i] = lo;
+        sumMin += lo;
+        cells += (double)d[0] * d[1] * d[2];
+    }
+    if (sumMin > cap) return false;
+    long long sum = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const double share = (double)dims[i][0] * dims[i][1] * dims[i][2] / cells;
+        t[i] = std::max(mins[i], (int)std::floor(share * cap));
+        sum += t[i];
+    }
+    while (sum > cap) {  // give back CTAs from the member with the most to spare
+        size_t j = 0;
+        for (size_t i = 1; i < n; ++i)
+            if (t[i] - mins[i] > t[j] - mins[j]) j = i;
+        --t[j];
+        --sum;
+    }
+    boxes->resize(n);
+    *smem = 0;
+    for (size_t i = 0; i < n; ++i) {
+        res_box(dims[i][0], dims[i][1], dims[i][2], t[i], &(*boxes)[i]);
+        *smem = std::max(*smem, (int)fx_res_smem_bytes(dims[i][0], (*boxes)[i].by, (*boxes)[i].bz));
+    }
+    return true;
 }
 
 // z chunk of the z-marching kernel when not chosen: the largest of 32, 16, 8 planes that
@@ -268,6 +352,20 @@ struct firex_sim {
         poisoned = true;
         err = std::string(what) + ": " + cudaGetErrorString(e);
         return FIREX_ERR_CUDA;
+    }
+
+    // After a stream synchronisation: whether a bounded device wait of this simulation
+    // expired (the resident Jacobi's group barrier). The fields are then incomplete.
+    int check_device_waits() {
+        unsigned word = 0;
+        cudaError_t e = cudaMemcpy(&word, h.sync + 2, sizeof(word), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return cuda_fail(e, "error word");
+        if (word != 0) {
+            poisoned = true;
+            err = "a bounded device wait expired (resident Jacobi barrier); the step did not complete";
+            return FIREX_ERR_TIMEOUT;
+        }
+        return FIREX_OK;
     }
 
     void* alloc(size_t nbytes) {
@@ -394,6 +492,9 @@ struct firex_batch {
     bool lastGraph = false;
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;  // batch override (AUTO: first member's)
     int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
+    int tableRes = -1;                               // whether resident boxes were requested
+    bool resOk = false;                              // ... and the batch fits one resident launch
+    int resSmem = 0;
     std::string err;
 
     // per-pass profiling (events between passes; graphs are bypassed while profiling)
@@ -417,9 +518,16 @@ struct firex_batch {
     }
 
     // Fills the brick prefix sums for the launch shape (k, zc).
-    void fill_table(int k, int zc, int zmZc) {
-        int acc[FX_NSHAPES] = {0, 0, 0, 0, 0};
+    void fill_table(int k, int zc, int zmZc, bool wantRes) {
+        int acc[FX_NSHAPES] = {};
         h->nsims = (int)members.size();
+        std::vector<FxResBox> boxes;
+        resOk = false;
+        if (wantRes && !members.empty()) {
+            std::vector<std::array<int, 3>> dims;
+            for (firex_sim* s : members) dims.push_back({s->X, s->Y, s->Z});
+            resOk = res_assign(dims, fx_res_capacity(members[0]->half), &boxes, &resSmem);
+        }
         for (size_t i = 0; i < members.size(); ++i) {
             firex_sim* s = members[i];
             h->sims[i] = s->d;
@@ -428,6 +536,11 @@ struct firex_batch {
             h->start[FX_SHAPE_COL][i] = acc[FX_SHAPE_COL];
             h->start[FX_SHAPE_ZM][i] = acc[FX_SHAPE_ZM];
             h->start[FX_SHAPE_TAB][i] = acc[FX_SHAPE_TAB];
+            h->start[FX_SHAPE_RES][i] = acc[FX_SHAPE_RES];
+            if (resOk) {
+                h->res[i] = boxes[i];
+                acc[FX_SHAPE_RES] += boxes[i].nby * boxes[i].nbz;
+            }
             acc[FX_SHAPE_TAB] += (fx_tab_layout(s->X, s->Y, s->Z).total + 255) / 256;
             acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z);
             acc[FX_SHAPE_ROW4] += (int)bricks_row4(s->X, s->Y, s->Z);
@@ -441,6 +554,7 @@ struct firex_batch {
         tableK = k;
         tableZc = zc;
         tableZmZc = zmZc;
+        tableRes = wantRes ? 1 : 0;
         tableDirty = true;
     }
 
@@ -464,7 +578,10 @@ struct firex_batch {
         int k = own ? jacobiK : members[0]->jacobiK;
         int zc = own ? jacobiZc : members[0]->jacobiZc;
         int dzc = 32;
-        if (kernel == FIREX_JACOBI_AUTO) default_jacobi(cells, &kernel, &dzc);
+        // AUTO and RESIDENT try the resident launch first; the single-sweep default is
+        // the fallback when the batch does not fit on chip
+        const bool wantRes = kernel == FIREX_JACOBI_AUTO || kernel == FIREX_JACOBI_RESIDENT;
+        if (kernel == FIREX_JACOBI_AUTO || kernel == FIREX_JACOBI_RESIDENT) default_jacobi(cells, &kernel, &dzc);
         if (kernel != FIREX_JACOBI_FUSED || (k != 2 && k != 3 && k != 4 && k != 6)) k = 1;
         long long zm32 = 0, zm16 = 0;
         for (firex_sim* s : members) {
@@ -478,7 +595,14 @@ struct firex_batch {
         if (!p.fuseP && !p.fuseR) p.k = 1;
         p.row4 = kernel == FIREX_JACOBI_UNBLOCKED;
         p.zmZc = (kernel == FIREX_JACOBI_ZMARCH && zc > 0) ? zc : zm_chunk(zm32, zm16);
-        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc) fill_table(p.k, p.zc, p.zmZc);
+        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 1 : 0))
+            fill_table(p.k, p.zc, p.zmZc, wantRes);
+        p.res = wantRes && resOk;
+        if (p.res) {
+            p.resSmem = resSmem;
+            p.k = 1;
+            p.fuseP = p.fuseR = false;
+        }
         for (int j = 0; j < FX_NSHAPES; ++j) p.bricks[j] = h->total[j];
         return p;
     }
@@ -856,7 +980,8 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
          (h.tab = (float*)s->alloc(s->table_bytes())) &&
          (s->d = (FxSimDev*)s->alloc(sizeof(FxSimDev))) &&
          (s->d_partial = (double*)s->alloc(2 * sizeof(double) * (size_t)fx_norm_partial_blocks(N))) &&
-         (s->d_norm = (double*)s->alloc(2 * sizeof(double)));
+         (s->d_norm = (double*)s->alloc(2 * sizeof(double))) && (h.sync = (unsigned*)s->alloc(FX_RES_SYNC_WORDS * 4)) &&
+         cudaMemset(h.sync, 0, FX_RES_SYNC_WORDS * 4) == cudaSuccess;
     if (!ok) {
         if (g_create_error.empty() || s->solo) g_create_error = "device allocation failed (" + std::to_string(need) + " bytes requested)";
         s->release();
@@ -933,7 +1058,7 @@ int firex_sync(firex_sim* s) {
     DeviceGuard dg(s->device);
     cudaError_t e = cudaStreamSynchronize(s->stream());
     if (e != cudaSuccess) return s->cuda_fail(e, "sync");
-    return FIREX_OK;
+    return s->check_device_waits();
 }
 
 // Device buffer and element size backing a field in the current parity, for direct copies.
@@ -1129,11 +1254,13 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
     out->launches_per_step = 8 + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+    out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
+                               : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     return FIREX_OK;
 }
 
 static bool jacobi_args_ok(int32_t kernel, int32_t block, int32_t zchunk) {
-    if (kernel < FIREX_JACOBI_AUTO || kernel > FIREX_JACOBI_FUSED || zchunk < 0 || zchunk > 4096) return false;
+    if (kernel < FIREX_JACOBI_AUTO || kernel > FIREX_JACOBI_RESIDENT || zchunk < 0 || zchunk > 4096) return false;
     return kernel != FIREX_JACOBI_FUSED || block == 2 || block == 3 || block == 4 || block == 6;
 }
 
@@ -1247,6 +1374,10 @@ int firex_batch_sync(firex_batch* b) {
     DeviceGuard dg(b->device);
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return b->poison(e, "batch sync");
+    for (firex_sim* s : b->members) {
+        const int rc = s->check_device_waits();
+        if (rc != FIREX_OK) return b->fail(rc, s->err);
+    }
     return FIREX_OK;
 }
 

@@ -13,6 +13,7 @@
 #include <cstdlib>
 
 #include "fx_internal.h"
+#include "fx_jacobi_res.cuh"
 #include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
 #include "fx_step_math.cuh"
@@ -25,6 +26,12 @@ namespace {
 // FireXEngine.ts:2049) and the per-step emission jitter (extension): splitmix64 of the
 // frame index, 24 random bits, same operations as the host.
 __global__ void fxk_step_begin(FxBatchDev* __restrict__ B) {
+    // the resident Jacobi's per-box flags start every step at zero (one CTA per simulation)
+    for (int s = blockIdx.x; s < B->nsims; s += gridDim.x) {
+        FxSimDev* S = B->sims[s];
+        for (int i = threadIdx.x; i < 2 * FX_RES_MAX_CTAS; i += blockDim.x) S->sync[FX_RES_FLAGS + i] = 0u;
+    }
+    if (blockIdx.x != 0) return;
     for (int s = threadIdx.x; s < B->nsims; s += blockDim.x) {
         FxSimDev* S = B->sims[s];
         if (!S->active) continue;
@@ -160,30 +167,6 @@ __global__ void __launch_bounds__(256) fxk_divergence(const FxBatchDev* __restri
 // starts from zero); phase 1: residual pressure, sweep `sweep` of R, starting from zero.
 // A sweep whose input is known to be zero skips its loads: ((wx*(0+0) + ...) - div)/D is
 // exactly (0 - div)/D. Storage PT is float or half; the update is FP32.
-// Buffers of launch `launch` of a solve phase: launches alternate between the two
-// buffers of the phase starting from the warm-start parity (primary, branches A and B)
-// or from buffer 0 (residual, and the cold primary of branch C); the first launch of a
-// cleared solve has a zero input.
-struct FxSolveBufs {
-    const void* pin;
-    void* pout;
-    bool zeroIn;
-};
-FXD FxSolveBufs fx_solve_bufs(const FxSimDev& S, int phase, int launch) {
-    FxSolveBufs r;
-    if (phase == 0) {
-        const int base = (S.mode == FIREX_PRESSURE_COLD_F32) ? 0 : S.pi;
-        r.pin = S.p[(base + launch) & 1];
-        r.pout = S.p[(base + launch + 1) & 1];
-        r.zeroIn = S.mode == FIREX_PRESSURE_COLD_F32 && launch == 0;
-    } else {
-        r.pin = S.corr[launch & 1];
-        r.pout = S.corr[(launch + 1) & 1];
-        r.zeroIn = launch == 0;
-    }
-    return r;
-}
-
 template <typename PT>
 __global__ void __launch_bounds__(256) fxk_jacobi(const FxBatchDev* __restrict__ B, int phase, int launch, int sweep) {
     fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
@@ -439,6 +422,19 @@ __global__ void __launch_bounds__(256) fxk_norm_partial(const FxSimDev* __restri
     }
 }
 
+// ---- every sweep of a Jacobi phase in one cooperative launch (fx_jacobi_res.cuh) --------
+template <typename PT>
+__global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatchDev* __restrict__ B, int phase) {
+    extern __shared__ float4 fx_res_smem[];
+    const int w = blockIdx.x;
+    if (w >= B->total[FX_SHAPE_RES]) return;
+    const int si = fx_find_sim(B->start[FX_SHAPE_RES], B->nsims, w);
+    const FxSimDev& S = *B->sims[si];
+    if (!S.active) return;
+    fx_res_box<PT, sizeof(PT) == 2>(S, B->res[si], w - B->start[FX_SHAPE_RES][si], phase,
+                                    reinterpret_cast<float*>(fx_res_smem));
+}
+
 __global__ void fxk_norm_final(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
     __shared__ double s_ss[256], s_mx[256];
     const int t = threadIdx.x;
@@ -500,7 +496,7 @@ static int persistent_grid(const void* kernel, int threads, int bricks) {
     return (int)(g < 1 ? 1 : g);
 }
 
-void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B) { fxk_step_begin<<<1, 256, 0, s>>>(B); }
+void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B) { fxk_step_begin<<<32, 256, 0, s>>>(B); }
 void fx_launch_step_end(cudaStream_t s, FxBatchDev* B) { fxk_step_end<<<1, 256, 0, s>>>(B); }
 void fx_launch_step_tables(cudaStream_t s, const FxBatchDev* B, int bricks) {
     fxk_step_tables<<<bricks > 0 ? bricks : 1, 256, 0, s>>>(B);
@@ -580,6 +576,39 @@ bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, 
         case 6: launch_tb_k<6>(s, pmode, B, bricks, phase, launch, zc); return true;
     }
     return false;
+}
+
+// Largest resident-Jacobi grid that one cooperative launch can keep resident.
+int fx_res_capacity(bool half) {
+    const void* fn = half ? (const void*)fxk_jacobi_res<__half> : (const void*)fxk_jacobi_res<float>;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FX_RES_THREADS, FX_RES_SMEM_MAX) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm * num_sms();
+}
+
+cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, const FxBatchDev* B, int ctas, int phase, int smem) {
+    const void* fn = half ? (const void*)fxk_jacobi_res<__half> : (const void*)fxk_jacobi_res<float>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)ctas);
+    cfg.blockDim = dim3(FX_RES_THREADS);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (half) return cudaLaunchKernelEx(&cfg, fxk_jacobi_res<__half>, B, phase);
+    return cudaLaunchKernelEx(&cfg, fxk_jacobi_res<float>, B, phase);
 }
 
 void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase) {

@@ -15,31 +15,28 @@
 // processor", IBM J. Res. Dev. 34(1), 1990): q = RN(x*rcp), e = x - q*d exactly by one
 // fused multiply-add, result RN(q + e*rcp). The theorem assumes no underflow, so the
 // step is used for 2^-96 <= |x| <= FLT_MAX (the quotient stays normal for any d below
-// 2^30); zeros (whose sign must survive) and tiny x take the IEEE division, and
-// x = +-inf or NaN, whose IEEE quotient by a finite d > 0 is x itself, is returned. The
-// engine enables this path for a given d only after checking on the device that it
-// equals IEEE x/d for every float x.
-FXD float fx_div_by_const(float x, float d, float rcp) {
+// 2^30); zeros (whose sign must survive) are returned as they are, tiny x take the IEEE
+// division, and x = +-inf or NaN, whose IEEE quotient by a finite d > 0 is x itself, is
+// returned. fx_div_range takes an explicit range [lo, hi] of |x| (divisors below 1 need
+// hi < FLT_MAX so that x * rcp cannot overflow). The engine enables this path for a
+// given (d, lo, hi) only after checking on the device that it equals IEEE x/d for every
+// float x.
+//
+// Out-of-range operands (tiny nonzero, |x| above the range, inf, NaN): kept out of line
+// so that the common path is three instructions and a compare, not a predicated IEEE
+// division.
+static __device__ __noinline__ float fx_div_rare(float x, float d) { return fabsf(x) <= 3.402823466e38f ? __fdiv_rn(x, d) : x; }
+
+FXD float fx_div_range(float x, float d, float rcp, float lo, float hi) {
+    const float q = __fmul_rn(x, rcp);
+    const float e = __fmaf_rn(-q, d, x);
+    float r = __fmaf_rn(e, rcp, q);
     const float ax = fabsf(x);
-    if (ax >= 1.2621774483536189e-29f && ax <= 3.402823466e38f) {  // 2^-96 .. FLT_MAX
-        const float q = __fmul_rn(x, rcp);
-        const float e = __fmaf_rn(-q, d, x);
-        return __fmaf_rn(e, rcp, q);
-    }
-    return ax <= 3.402823466e38f ? __fdiv_rn(x, d) : x;
+    if (!(ax >= lo && ax <= hi)) r = (x == 0.0f) ? x : fx_div_rare(x, d);  // a zero keeps its sign
+    return r;
 }
 
-// The same step on an explicit range [lo, hi] of |x| (divisors below 1 need hi < FLT_MAX
-// so that x * rcp cannot overflow); outside it IEEE division, or x for inf and NaN.
-FXD float fx_div_range(float x, float d, float rcp, float lo, float hi) {
-    const float ax = fabsf(x);
-    if (ax >= lo && ax <= hi) {
-        const float q = __fmul_rn(x, rcp);
-        const float e = __fmaf_rn(-q, d, x);
-        return __fmaf_rn(e, rcp, q);
-    }
-    return ax <= 3.402823466e38f ? __fdiv_rn(x, d) : x;
-}
+FXD float fx_div_by_const(float x, float d, float rcp) { return fx_div_range(x, d, rcp, 1.2621774483536189e-29f, 3.402823466e38f); }
 
 // x / c.d, by the checked constant-divisor path when the engine enabled it.
 FXD float fx_divc(float x, const FxDivc& c) { return c.ok ? fx_div_range(x, c.d, c.rcp, c.lo, c.hi) : __fdiv_rn(x, c.d); }

@@ -270,7 +270,7 @@ class FireXSim(_Handle):
 
 
 JACOBI_KERNELS = {"auto": A.JACOBI_AUTO, "unblocked": A.JACOBI_UNBLOCKED, "zmarch": A.JACOBI_ZMARCH,
-                  "fused": A.JACOBI_FUSED}
+                  "fused": A.JACOBI_FUSED, "resident": A.JACOBI_RESIDENT}
 
 
 def jacobi_kernel(kernel) -> int:

@@ -250,6 +250,10 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
 #define FIREX_JACOBI_UNBLOCKED 1
 #define FIREX_JACOBI_ZMARCH 2
 #define FIREX_JACOBI_FUSED 3
+/* Every sweep of a phase in one cooperative launch with the pressure held in shared
+ * memory (only box faces cross L2 between sweeps); used by AUTO whenever the batch fits
+ * on chip, else the single-sweep default runs. */
+#define FIREX_JACOBI_RESIDENT 4
 int firex_set_jacobi(firex_sim* sim, int32_t kernel, int32_t block, int32_t zchunk);
 int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, int32_t zchunk);
 
@@ -260,7 +264,8 @@ typedef struct firex_diagnostics {
     int32_t jacobi_zchunk;    /* z planes per CTA of the Jacobi launches */
     int32_t graph;            /* 1: steps replay a captured CUDA graph */
     int32_t launches_per_step;
-    int32_t reserved[11];
+    int32_t jacobi_kernel;    /* FIREX_JACOBI_* kernel the last step ran */
+    int32_t reserved[10];
 } firex_diagnostics;
 int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
 
