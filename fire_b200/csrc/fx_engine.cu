@@ -382,7 +382,7 @@ struct firex_sim {
     static size_t planned_bytes(int X, int Y, int Z, int storage, int mode) {
         const long long N = (long long)X * Y * Z;
         const size_t species = storage == FX_STORAGE_MIXED ? 8 : 16;
-        const size_t pbytes = (storage == FX_STORAGE_MIXED || mode == FIREX_PRESSURE_F16) ? 2 : 4;
+        const size_t pbytes = mode == FIREX_PRESSURE_F16 ? 2 : 4;
         const size_t npress = mode == FIREX_PRESSURE_COLD_F32 ? 2 : 4;
         const size_t per = 16 * 2 + species * 2 + pbytes * npress + 4 /*div*/ + 4 /*reaction*/ + 4 /*liquid*/ + 4 /*tmp*/;
         return (size_t)N * per + (size_t)fx_tab_layout(X, Y, Z).total * 4 + sizeof(FxSimDev) + 64 * 1024;
@@ -563,7 +563,7 @@ struct firex_batch {
         if (members.empty()) return p;
         p.storage = members[0]->storage;
         p.half = members[0]->half;
-        p.pmode = !p.half ? FX_TB_F32 : (p.storage == FX_STORAGE_F32 ? FX_TB_F16_ROUND : FX_TB_F16);
+        p.pmode = p.half ? FX_TB_F16_ROUND : FX_TB_F32;
         bool uniformP = true, uniformR = true;
         long long cells = 0;
         for (firex_sim* s : members) {
@@ -912,10 +912,6 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
     const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
-    if (storage == FX_STORAGE_MIXED && mode == FIREX_PRESSURE_COLD_F32) {
-        g_create_error = "mixed precision stores pressure in FP16; the cold f32 branch does not apply";
-        return FIREX_ERR_UNSUPPORTED;
-    }
     const size_t need = firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode);
     if (opt->memory_budget_bytes && need > opt->memory_budget_bytes) {
         g_create_error = "grid needs " + std::to_string(need) + " device bytes, above the " +
@@ -931,7 +927,7 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
     s->opt = *opt;
     s->mode = mode;
     s->storage = storage;
-    s->half = storage == FX_STORAGE_MIXED || mode == FIREX_PRESSURE_F16;
+    s->half = mode == FIREX_PRESSURE_F16;
     for (int i = 0; i < kNumParams; ++i) s->named[i] = kParams[i].def;
     if (opt->jacobi_block > 1) {
         s->jacobiKernel = FIREX_JACOBI_FUSED;

@@ -155,9 +155,7 @@ FXD void fx_res_box(const FxSimDev& S, const FxResBox& bx, int b, int phase, flo
     const bool hasL = x0 > 0, hasR = x0 + 4 < X;
     const bool faceY = (ly == 0 && nbLoY) || (ly == ny - 1 && nbHiY);
     const long long gRow = (long long)(z0 + zs) * XY + (long long)y * X + x0;  // global index of (x0, y, z0+zs)
-    const FxJacobiConst c{S.jc[0], S.jc[1], S.jc[2], S.jc[3]};
-    const float rcpD = S.jcRcp;
-    const bool fastDiv = S.jcFastDiv != 0;
+    const FxJacobiConst2 c2 = fx_jacobi_const2(FxJacobiConst{S.jc[0], S.jc[1], S.jc[2], S.jc[3]}, S.jcRcp, S.jcFastDiv != 0);
     __syncthreads();
 
     for (int s = 0; s < n; ++s) {
@@ -175,17 +173,10 @@ FXD void fx_res_box(const FxSimDev& S, const FxResBox& bx, int b, int phase, flo
                     const float pl = hasL ? sp[off - 1] : pc.x;
                     const float pr = hasR ? sp[off + 4] : pc.w;
                     const float4 d = *reinterpret_cast<const float4*>(sd + offD + k * planeD);
-                    float o[4];
-                    o[0] = fx_jacobi_numerator(c, pl, pc.y, pb.x, pt.x, pk.x, pf.x, d.x);
-                    o[1] = fx_jacobi_numerator(c, pc.x, pc.z, pb.y, pt.y, pk.y, pf.y, d.y);
-                    o[2] = fx_jacobi_numerator(c, pc.y, pc.w, pb.z, pt.z, pk.z, pf.z, d.z);
-                    o[3] = fx_jacobi_numerator(c, pc.z, pr, pb.w, pt.w, pk.w, pf.w, d.w);
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        o[i] = fastDiv ? fx_div_by_const(o[i], c.denom, rcpD) : __fdiv_rn(o[i], c.denom);
-                        if (ROUND) o[i] = PStore<__half>::round(o[i]);
-                    }
-                    nv[k] = top ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : make_float4(o[0], o[1], o[2], o[3]);
+                    float4 o = fx_jacobi4(c2, pl, pc, pr, pb, pt, pk, pf, d);
+                    if (ROUND) o = make_float4(PStore<__half>::round(o.x), PStore<__half>::round(o.y),
+                                               PStore<__half>::round(o.z), PStore<__half>::round(o.w));
+                    nv[k] = top ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : o;
                     pk = pc;
                     pc = pf;
                 }

@@ -456,6 +456,91 @@ FXD float fx_jacobi_numerator(const FxJacobiConst& c, float l, float r, float b,
                                __fmul_rn(c.wz, __fadd_rn(k, f))),
                      div);
 }
+// ---- packed FP32 pairs (add/sub/mul/fma .rn.f32x2, Blackwell): each lane is rounded
+// exactly as the scalar IEEE operation, so pairing changes no result bit.
+typedef unsigned long long fx_f2;
+FXD fx_f2 fx_pack2(float a, float b) {
+    fx_f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+FXD float2 fx_unpack2(fx_f2 v) {
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return make_float2(a, b);
+}
+FXD fx_f2 fx_add2(fx_f2 a, fx_f2 b) {
+    fx_f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+FXD fx_f2 fx_sub2(fx_f2 a, fx_f2 b) {
+    fx_f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+FXD fx_f2 fx_mul2(fx_f2 a, fx_f2 b) {
+    fx_f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+FXD fx_f2 fx_fma2(fx_f2 a, fx_f2 b, fx_f2 c) {
+    fx_f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
+// Jacobi constants as pairs, for fx_jacobi4.
+struct FxJacobiConst2 {
+    fx_f2 rcp, negDenom;
+    float wxS, wyS, wzS, denom, rcpS;
+    bool fast;
+};
+FXD FxJacobiConst2 fx_jacobi_const2(const FxJacobiConst& c, float rcp, bool fast) {
+    return FxJacobiConst2{fx_pack2(rcp, rcp), fx_pack2(-c.denom, -c.denom), c.wx, c.wy, c.wz, c.denom, rcp, fast};
+}
+
+// Four consecutive x cells of one Jacobi sweep (the operations of fx_jacobi_numerator and
+// fx_div_by_const, cell by cell, two cells per instruction): pc holds the cells, l and r
+// their outer x neighbours, pb/pt/pk/pf the y-1, y+1, z-1, z+1 rows, d the divergence.
+FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, float4 pb, float4 pt, float4 pk, float4 pf,
+                      float4 d) {
+    const fx_f2 mid = fx_pack2(pc.y, pc.z);
+    const fx_f2 lr01 = fx_add2(fx_pack2(l, pc.x), mid);
+    const fx_f2 lr23 = fx_add2(mid, fx_pack2(pc.w, r));
+    const fx_f2 bt01 = fx_add2(fx_pack2(pb.x, pb.y), fx_pack2(pt.x, pt.y));
+    const fx_f2 bt23 = fx_add2(fx_pack2(pb.z, pb.w), fx_pack2(pt.z, pt.w));
+    const fx_f2 kf01 = fx_add2(fx_pack2(pk.x, pk.y), fx_pack2(pf.x, pf.y));
+    const fx_f2 kf23 = fx_add2(fx_pack2(pk.z, pk.w), fx_pack2(pf.z, pf.w));
+    // The weight products stay scalar: a packed multiply feeding a packed add is contracted
+    // into a packed fma by the code generator (measured on B200), which rounds once instead
+    // of twice. Scalar mul.rn is never contracted.
+    const float2 s01 = fx_unpack2(lr01), s23 = fx_unpack2(lr23), u01 = fx_unpack2(bt01), u23 = fx_unpack2(bt23);
+    const float2 v01 = fx_unpack2(kf01), v23 = fx_unpack2(kf23);
+    const fx_f2 x01 = fx_pack2(__fmul_rn(c.wxS, s01.x), __fmul_rn(c.wxS, s01.y));
+    const fx_f2 x23 = fx_pack2(__fmul_rn(c.wxS, s23.x), __fmul_rn(c.wxS, s23.y));
+    const fx_f2 y01 = fx_pack2(__fmul_rn(c.wyS, u01.x), __fmul_rn(c.wyS, u01.y));
+    const fx_f2 y23 = fx_pack2(__fmul_rn(c.wyS, u23.x), __fmul_rn(c.wyS, u23.y));
+    const fx_f2 z01 = fx_pack2(__fmul_rn(c.wzS, v01.x), __fmul_rn(c.wzS, v01.y));
+    const fx_f2 z23 = fx_pack2(__fmul_rn(c.wzS, v23.x), __fmul_rn(c.wzS, v23.y));
+    const fx_f2 n01 = fx_sub2(fx_add2(fx_add2(x01, y01), z01), fx_pack2(d.x, d.y));
+    const fx_f2 n23 = fx_sub2(fx_add2(fx_add2(x23, y23), z23), fx_pack2(d.z, d.w));
+    const float2 a = fx_unpack2(n01), b = fx_unpack2(n23);
+    if (!c.fast) return make_float4(__fdiv_rn(a.x, c.denom), __fdiv_rn(a.y, c.denom), __fdiv_rn(b.x, c.denom), __fdiv_rn(b.y, c.denom));
+    // Markstein's step on both pairs: q = x rcp, e = fma(q, -d, x) = x - q d, q + e rcp
+    const fx_f2 q01 = fx_mul2(n01, c.rcp), q23 = fx_mul2(n23, c.rcp);
+    const fx_f2 r01 = fx_fma2(fx_fma2(q01, c.negDenom, n01), c.rcp, q01);
+    const fx_f2 r23 = fx_fma2(fx_fma2(q23, c.negDenom, n23), c.rcp, q23);
+    const float2 ra = fx_unpack2(r01), rb = fx_unpack2(r23);
+    // every |x| inside [2^-96, FLT_MAX] (bit patterns 0x0f800000 .. 0x7f7fffff)?
+    const unsigned lo = 0x0f800000u, span = 0x7f7fffffu - 0x0f800000u;
+    const bool ok = ((__float_as_uint(a.x) & 0x7fffffffu) - lo <= span) & ((__float_as_uint(a.y) & 0x7fffffffu) - lo <= span) &
+                    ((__float_as_uint(b.x) & 0x7fffffffu) - lo <= span) & ((__float_as_uint(b.y) & 0x7fffffffu) - lo <= span);
+    if (ok) return make_float4(ra.x, ra.y, rb.x, rb.y);
+    return make_float4(fx_div_by_const(a.x, c.denom, c.rcpS), fx_div_by_const(a.y, c.denom, c.rcpS),
+                       fx_div_by_const(b.x, c.denom, c.rcpS), fx_div_by_const(b.y, c.denom, c.rcpS));
+}
+
 FXD float fx_jacobi_update(const FxJacobiConst& c, float l, float r, float b, float t, float k, float f, float div) {
     return __fdiv_rn(fx_jacobi_numerator(c, l, r, b, t, k, f, div), c.denom);
 }

@@ -138,8 +138,11 @@ def maximumFireXDeviceDenseCubeAxis(limits: dict) -> int:
 
 
 def device_bytes_per_cell(precision: int = A.PRECISION_F32, pressure_mode: int = A.PRESSURE_WARM_F32) -> int:
-    """Bytes per cell this library allocates for one simulation (engine planned_bytes)."""
-    if precision == A.PRECISION_MIXED:
-        return 96
-    base = 16 * 4 + 4 * 2 + 4 + 4
-    return base + (16 if pressure_mode == A.PRESSURE_WARM_F32 else 8)
+    """Bytes per cell this library allocates for one simulation (the engine's planned_bytes
+    without its per-simulation constant): flow ping-pong, species ping-pong (FP16 when
+    mixed), pressure + residual pressure buffers (FP16 in branch B; the cold branch shares
+    one pair), divergence, reaction, liquid and one scratch field."""
+    species = 8 if precision == A.PRECISION_MIXED else 16
+    pbytes = 2 if pressure_mode == A.PRESSURE_F16 else 4
+    npress = 2 if pressure_mode == A.PRESSURE_COLD_F32 else 4
+    return 16 * 2 + species * 2 + pbytes * npress + 4 * 4

@@ -36,9 +36,12 @@ extern "C" {
 
 /* ---- options ---------------------------------------------------------------------- */
 /* Storage precision of the step. F32 mirrors the reference's f32 storage buffers;
- * MIXED stores transported scalars (T, species) and the residual (correction) pressure
- * in FP16 and keeps velocity, divergence and the primary pressure in FP32; all
- * arithmetic is FP32. */
+ * MIXED stores the transported species (fuel, O2, products, vapor) in FP16 (RNE) and keeps
+ * velocity and temperature (one 16-byte record), divergence and reaction in FP32; all
+ * arithmetic is FP32 and norms are FP64. Pressure storage follows the pressure branch
+ * (FP16 only in branch B). Against the FP64 oracle, FP32 arithmetic itself leaves the
+ * post-projection divergence 4e-5 .. 9e-5 of the pre-projection norm away; FP16 species
+ * move that by under 1e-6, FP16 pressure (branch B) raises it to 4e-3 .. 8e-3. */
 #define FIREX_PRECISION_F32 0
 #define FIREX_PRECISION_MIXED 1
 

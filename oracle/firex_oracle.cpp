@@ -646,6 +646,10 @@ struct SimBase {
     virtual int read_field(int field, void* out, size_t bytes) = 0;
     virtual int write_field(int field, const void* in, size_t bytes) = 0;
     virtual void divergence_norm(double out[3]) = 0;
+    // Divergence of the predicted flow (before the first projection) of the last step over
+    // interior cells: L2, max abs, cell count. The accuracy metric of mixed precision
+    // normalises divergence differences by this L2 norm of the FP64 step.
+    double preDiv[3] = {0, 0, 0};
 };
 
 template <typename T>
@@ -721,6 +725,7 @@ struct Sim : SimBase {
                       reaction.data());
         speciesIndex = 1 - s;
         divergence_pass(g, flow[1].data(), divergence.data());
+        interior_norm(divergence.data(), preDiv);
         const int P = opt.pressure_iterations, R = opt.correction_iterations;
         if (mode == FIREX_PRESSURE_WARM_F32) {  // branch A (FireXEngine.ts:2248-2273)
             for (int i = 0; i < P; ++i) {
@@ -885,6 +890,22 @@ struct Sim : SimBase {
         return FIREX_ERR_BAD_ARG;
     }
 
+    // L2 and max abs of a cell field over interior cells (the one-cell shell excluded).
+    void interior_norm(const T* d, double out[3]) const {
+        double ss = 0, mx = 0, n = 0;
+        for (int z = 1; z < Z - 1; ++z)
+            for (int y = 1; y < Y - 1; ++y)
+                for (int x = 1; x < X - 1; ++x) {
+                    const double v = (double)d[(size_t)x + (size_t)X * ((size_t)y + (size_t)Y * z)];
+                    ss += v * v;
+                    mx = std::max(mx, std::fabs(v));
+                    n += 1;
+                }
+        out[0] = std::sqrt(ss);
+        out[1] = mx;
+        out[2] = n;
+    }
+
     void divergence_norm(double out[3]) override {
         std::vector<T> d(N);
         Grid<T> g = grid(0.0);
@@ -1009,6 +1030,11 @@ int fxo_divergence_norm(void* h, double out[3]) {
 }
 
 int fxo_pressure_mode(void* h) { return ((SimBase*)h)->mode; }
+
+int fxo_pre_projection_norm(void* h, double out[3]) {
+    for (int i = 0; i < 3; ++i) out[i] = ((SimBase*)h)->preDiv[i];
+    return FIREX_OK;
+}
 
 float fxo_emission_jitter(uint64_t seed, int64_t frame, float a) { return emission_jitter(seed, frame, a); }
 float fxo_velocity_noise(uint64_t seed, uint64_t cell, int comp, float a) { return velocity_noise(seed, cell, comp, a); }

@@ -53,6 +53,7 @@ def load() -> C.CDLL:
             "fxo_get_uniforms": (C.c_int, [vp, C.c_double, C.POINTER(C.c_float)]),
             "fxo_divergence_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
             "fxo_pressure_mode": (C.c_int, [vp]),
+            "fxo_pre_projection_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
             "fxo_emission_jitter": (C.c_float, [C.c_uint64, C.c_int64, C.c_float]),
             "fxo_velocity_noise": (C.c_float, [C.c_uint64, C.c_uint64, C.c_int, C.c_float]),
             "fxo_f32_to_f16": (C.c_uint16, [C.c_float]),
@@ -93,6 +94,12 @@ class OracleSim(_Handle):
     @property
     def pressure_mode(self) -> int:
         return self._lib.fxo_pressure_mode(self._h)
+
+    def pre_projection_norm(self) -> tuple[float, float, int]:
+        """Interior divergence of the last step's predicted flow: (L2, max abs, cells)."""
+        out = (C.c_double * 3)()
+        self._lib.fxo_pre_projection_norm(self._h, out)
+        return out[0], out[1], int(out[2])
 
 
 def num_threads() -> int:

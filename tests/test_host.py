@@ -188,3 +188,20 @@ def test_create_rejects_bad_arguments_without_a_device():
     o.memory_budget_bytes = 1024
     assert lib.firex_create(A.DIMS(64, 96, 64), C.byref(o), C.byref(h)) == A.ERR_BUDGET
     assert not h.value
+
+
+def test_device_bytes_per_cell_matches_library_plan():
+    """The Python memory model (admission by budget) and the library's plan agree up to the
+    per-simulation constant (per-step tables, descriptor, scratch)."""
+    lib = load_library()
+    combos = [(A.PRECISION_F32, A.PRESSURE_WARM_F32), (A.PRECISION_F32, A.PRESSURE_F16),
+              (A.PRECISION_F32, A.PRESSURE_COLD_F32), (A.PRECISION_MIXED, A.PRESSURE_WARM_F32),
+              (A.PRECISION_MIXED, A.PRESSURE_F16)]
+    for precision, mode in combos:
+        o = A.Options()
+        lib.firex_default_options(C.byref(o))
+        o.precision, o.pressure_mode = precision, mode
+        for dims in ((64, 96, 64), (128, 192, 128), (508, 508, 508)):
+            n = dims[0] * dims[1] * dims[2]
+            extra = lib.firex_planned_device_bytes(A.DIMS(*dims), C.byref(o)) - n * G.device_bytes_per_cell(precision, mode)
+            assert 0 <= extra < (1 << 24), (precision, mode, dims, extra)
