@@ -313,6 +313,174 @@ def run_gpu(args) -> None:
         dist.destroy_process_group()
 
 
+# ---- batched mixed precision: 48 uneven simulations stepped by shared launches --------------
+BATCH_FAMILY = [(64, 96, 64), (96, 144, 96), (128, 192, 128), (160, 240, 160)]
+
+
+def batch48_scenes(seed: int = 4242, count: int = 48):
+    """48 scenes drawn by seed: grid from the family, 1-3 sphere emitters of radius 6-24
+    cells at random positions near the floor, seeded noise and jitter."""
+    import random
+    rng = random.Random(seed)
+    out = []
+    for i in range(count):
+        dims = rng.choice(BATCH_FAMILY)
+        X, Y, Z = dims
+        spheres = []
+        for _ in range(rng.randint(1, 3)):
+            r = rng.uniform(6.0, min(24.0, X / 4))
+            spheres.append(dict(center=(rng.uniform(r, X - r), rng.uniform(2 + r / 2, Y / 5), rng.uniform(r, Z - r)),
+                                radius=r, fuel=1.0, temperature=1500.0))
+        out.append((dims, dict(pressure_iterations=96, correction_iterations=96, seed=rng.randrange(1 << 30),
+                               velocity_noise=0.05, emission_jitter=0.1, spheres=spheres)))
+    return out
+
+
+def run_batch48(args) -> None:
+    """Gcell-steps/s of the 48-simulation batch in mixed precision (one set of launches per
+    step for all members, graph-replayed) against the same 48 simulations stepped one at a
+    time in plain FP32, plus the post-projection divergence of every mixed member against
+    its plain FP32 twin (relative to the twin's pre-projection scale: the divergence of the
+    first step's predicted flow is not kept, so the plain post-projection norm is used)."""
+    import numpy as np
+    import torch
+
+    from fire_b200 import _abi as A
+    from fire_b200.sim import FireXBatch, FireXSim, make_options
+
+    torch.cuda.set_device(0)
+    scenes = batch48_scenes()
+    steps = args.steps
+    cells = [d[0] * d[1] * d[2] for d, _ in scenes]
+    total_cells = sum(cells)
+
+    # plain FP32, one simulation at a time (each on its own stream, its own step graph)
+    plain_ms = 0.0
+    plain_norms = []
+    for dims, o in scenes:
+        s = FireXSim(dims, make_options(**o))
+        st = torch.cuda.ExternalStream(s.stream)
+        s.step(args.warmup, DT)
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(steps, DT)
+        e1.record(st)
+        s.sync()
+        plain_ms += e0.elapsed_time(e1)
+        plain_norms.append(s.read("final_divergence"))
+        s.close()
+    plain = total_cells * steps / (plain_ms / 1e3) / 1e9
+
+    # batched, mixed precision
+    b = FireXBatch()
+    members = [FireXSim(dims, make_options(**{**o, "precision": A.PRECISION_MIXED})) for dims, o in scenes]
+    for m in members:
+        b.add(m)
+    st = torch.cuda.ExternalStream(b.stream)
+    b.step(args.warmup, DT)
+    b.sync()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    with ClockSampler(0) as clk:
+        evs[0].record(st)
+        for i in range(steps):
+            b.step(1, DT)
+            evs[i + 1].record(st)
+        b.sync()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    batch_ms = evs[0].elapsed_time(evs[-1])
+    batched = total_cells * steps / (batch_ms / 1e3) / 1e9
+    diag = members[0].diagnostics
+    # accuracy: final divergence of each mixed member against its plain FP32 twin
+    worst = 0.0
+    for m, ref in zip(members, plain_norms):
+        d = m.read("final_divergence")[1:-1, 1:-1, 1:-1].astype(np.float64)
+        r = ref[1:-1, 1:-1, 1:-1].astype(np.float64)
+        worst = max(worst, float(np.linalg.norm((d - r).ravel()) / max(np.linalg.norm(r.ravel()), 1e-300)))
+    b.close()
+    line = {
+        "metric": "Gcell-steps/s batched mixed vs plain FP32", "value": batched, "unit": METRIC, "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": batch_ms / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (species stored f16)", "data": "synthetic",
+        "config": {"workload": "48 simulations, grids by seed from 64x96x64 / 96x144x96 / 128x192x128 / 160x240x160, "
+                               "1-3 spheres r 6-24, 96+96 Jacobi, dt=1/60", "cells": total_cells,
+                   "grids": {str(d): sum(1 for x, _ in scenes if x == d) for d in BATCH_FAMILY},
+                   "l2": "inputs larger than L2"},
+        "plain_fp32_sequential": plain, "speedup_vs_plain": batched / plain,
+        "p50_step_ms": percentile(step_ms, 0.5), "p99_step_ms": percentile(step_ms, 0.99),
+        "jacobi_kernel": diag.get("jacobi_kernel"), "launches_per_step": diag.get("launches_per_step"),
+        "final_divergence_rel_l2_vs_plain_max": worst, "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- served stream: Poisson arrivals, admission by HBM budget, continuous batching -----------
+SERVE_FAMILY = [(64, 96, 64), (96, 144, 96), (128, 192, 128), (160, 240, 160), (192, 288, 192)]
+
+
+def run_serve(args) -> None:
+    """The served stream: Poisson arrivals at 40 requests/s, grids uniform over the family,
+    60-600 steps each, 150 GB budget, mixed precision, continuous batching; the arrival
+    window and the run are bounded by --serve-seconds. The same stream served plainly (one
+    request at a time, FP32, FIFO) for the same time is reported beside it."""
+    import torch
+
+    from fire_b200 import _abi as A
+    from fire_b200.serve import FireXServer, poisson_stream
+    from fire_b200.sim import FireXSim, make_options
+
+    torch.cuda.set_device(0)
+    window = float(args.serve_seconds)
+    stream = poisson_stream(40.0, window, SERVE_FAMILY, (60, 600), seed=777)
+    srv = FireXServer(budget_bytes=150 * 10**9, precision=A.PRECISION_MIXED)
+    srv.run_until_idle(list(stream), time_limit=window)
+    served = srv.stats()
+    srv.close()
+
+    # plain: FIFO, one request at a time in FP32, same arrivals, same wall budget
+    stream = poisson_stream(40.0, window, SERVE_FAMILY, (60, 600), seed=777)
+    t0 = time.perf_counter()
+    cell_steps, dev_ms, waits, steps_ms = 0, 0.0, [], []
+    done = 0
+    for r in stream:
+        now = time.perf_counter() - t0
+        if now > window:
+            break
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        waits.append(max(0.0, time.perf_counter() - t0 - r.arrival))
+        s = FireXSim(r.dims, make_options(**r.options))
+        st = torch.cuda.ExternalStream(s.stream)
+        n = 0
+        while n < r.steps and time.perf_counter() - t0 < window:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            s.step(1, r.dt)
+            e1.record(st)
+            s.sync()
+            ms = e0.elapsed_time(e1)
+            steps_ms.append(ms)
+            dev_ms += ms
+            n += 1
+        cell_steps += n * r.dims[0] * r.dims[1] * r.dims[2]
+        done += n == r.steps
+        s.close()
+    plain = {"gcell_steps_per_s_device": cell_steps / (dev_ms / 1e3) / 1e9 if dev_ms else None,
+             "p50_step_ms": percentile(steps_ms, 0.5) if steps_ms else None,
+             "p99_step_ms": percentile(steps_ms, 0.99) if steps_ms else None,
+             "p50_queue_wait_s": percentile(waits, 0.5) if waits else None,
+             "p99_queue_wait_s": percentile(waits, 0.99) if waits else None, "completed": done}
+    line = {
+        "metric": "served Gcell-steps/s, p50/p99 step ms", "value": served["gcell_steps_per_s_device"],
+        "unit": METRIC, "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (species stored f16)",
+        "data": "synthetic", "config": {"workload": f"Poisson 40 req/s over {window:.0f} s, grids uniform over "
+                                                    "64x96x64 .. 192x288x192, 60-600 steps, 150 GB budget",
+                                         "requests": len(stream)},
+        "served": served, "plain_fifo_fp32": plain,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -320,11 +488,19 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fire_b200", choices=["fire_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="hd", choices=["hd", "batch48", "serve"],
+                    help="hd: the headline HD step (default); batch48: 48 uneven simulations, batched mixed "
+                         "vs plain FP32; serve: Poisson-arrival serving")
+    ap.add_argument("--serve-seconds", type=float, default=30.0)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch48":
+        run_batch48(args)
+    elif args.workload == "serve":
+        run_serve(args)
     else:
         run_gpu(args)
 

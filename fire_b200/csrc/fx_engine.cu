@@ -676,6 +676,12 @@ struct firex_batch {
             *out = it->second;
             return cudaSuccess;
         }
+        // a serving batch changes membership often: keep a bounded set of step graphs
+        if (graphs.size() >= 16) {
+            cudaError_t w = cudaStreamSynchronize(stream);  // no replay of them is still in flight
+            if (w != cudaSuccess) return w;
+            drop_graphs();
+        }
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return e;

@@ -1,8 +1,9 @@
 // fx_jacobi_zm.cuh — one Jacobi sweep (solvePressureGlobal, shaders.ts:375-403) by
 // z-marching tiles with an asynchronous shared-memory pipeline.
 //
-// A CTA of 256 threads owns an x-y tile of 128 x 8 cells (lane: 4 consecutive x cells,
-// warp: one row) and walks a chunk of z planes. Pressure planes, with a one-row halo
+// A CTA of 256 threads owns an x-y tile of 1024 cells, 128 x 8, 64 x 16 or 32 x 32 (the
+// widest that wastes the fewest lanes on the simulation's X; a thread takes 4
+// consecutive x cells of one row) and walks a chunk of z planes. Pressure planes, with a one-row halo
 // above and below and a 4-cell halo segment left and right, and the divergence rows
 // stream into a ring of FX_ZM_SLOTS shared-memory slots through cp.async (16- or
 // 8-byte global->shared copies that need no registers), three planes ahead of the plane
@@ -20,20 +21,33 @@
 #include "fx_storage.cuh"
 
 #define FX_ZM_THREADS 256
-#define FX_ZM_TX 128  // tile cells in x (32 lanes x 4)
-#define FX_ZM_TY 8    // tile rows in y (8 warps)
+#define FX_ZM_CELLS 1024  // tile cells per plane: TX x TY = 128 x 8, 64 x 16 or 32 x 32
 #define FX_ZM_SLOTS 6
-#define FX_ZM_COLS (FX_ZM_TX + 8)  // 4-cell halo segment on each side
-#define FX_ZM_ROWS (FX_ZM_TY + 2)
+#define FX_ZM_PSLOT 1360  // pressure slot: (TY + 2) rows of (TX + 8) (largest of the three shapes)
+
+// Tile width for an X-cell row: the widest of 128, 64, 32 that wastes the fewest lanes
+// (X = 160 takes 32-wide tiles, X = 64 64-wide, X = 508 128-wide).
+__host__ __device__ inline int fx_zm_tile_w(int X) {
+    int best = 128, waste = ((X + 127) / 128) * 128 - X;
+    for (int w = 64; w >= 32; w /= 2) {
+        const int wst = ((X + w - 1) / w) * w - X;
+        if (wst < waste) {
+            best = w;
+            waste = wst;
+        }
+    }
+    return best;
+}
 
 __host__ __device__ inline int fx_zm_bricks(int X, int Y, int Z, int zc) {
-    return ((X + FX_ZM_TX - 1) / FX_ZM_TX) * ((Y + FX_ZM_TY - 1) / FX_ZM_TY) * ((Z + zc - 1) / zc);
+    const int tx = fx_zm_tile_w(X), ty = FX_ZM_CELLS / tx;
+    return ((X + tx - 1) / tx) * ((Y + ty - 1) / ty) * ((Z + zc - 1) / zc);
 }
 
 template <typename PT>
 struct FxZmSmem {
-    PT p[FX_ZM_SLOTS][FX_ZM_ROWS][FX_ZM_COLS];
-    float d[FX_ZM_SLOTS][FX_ZM_TY][FX_ZM_TX];
+    PT p[FX_ZM_SLOTS][FX_ZM_PSLOT];
+    float d[FX_ZM_SLOTS][FX_ZM_CELLS];
 };
 
 FXD void fx_cp_async16(void* smem, const void* gmem) {
@@ -57,32 +71,51 @@ FXD void fx_cp4(PT* smem, const PT* gmem) {
     else fx_cp_async8(smem, gmem);
 }
 
+// Tile geometry of one thread: TX cells wide (L = TX / 4 lanes of 4 cells per row), TY
+// rows; thread t takes row t / L and cell group t % L.
+struct FxZmGeom {
+    int tx, ty, cols;  // cols = TX + 8: a row with its 4-cell halo segments
+    int cg, row;       // this thread's cell group and row
+};
+template <int TX>
+FXD FxZmGeom fx_zm_geom() {
+    FxZmGeom g;
+    g.tx = TX;
+    g.ty = FX_ZM_CELLS / TX;
+    g.cols = TX + 8;
+    g.cg = threadIdx.x % (TX / 4);
+    g.row = threadIdx.x / (TX / 4);
+    return g;
+}
+
 // Issues the copies of plane q (clamped) into ring slot `slot`: the tile rows, the halo
 // rows and the halo segments (pressure), and the tile rows of the divergence when
 // withDiv (the plane is one the chunk updates).
 template <typename PT>
-FXD void fx_zm_issue(FxZmSmem<PT>& sm, int slot, const PT* __restrict__ p, const float* __restrict__ div, int X, int Y,
-                     int Z, int x0t, int y0t, int q, bool loadP, bool withDiv) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+FXD void fx_zm_issue(FxZmSmem<PT>& sm, const FxZmGeom& G, int slot, const PT* __restrict__ p, const float* __restrict__ div,
+                     int X, int Y, int Z, int x0t, int y0t, int q, bool loadP, bool withDiv) {
     const int qc = q < 0 ? 0 : (q > Z - 1 ? Z - 1 : q);
     const long long plane = (long long)qc * X * Y;
-    const int x = x0t + 4 * lane;
+    const int x = x0t + 4 * G.cg;
+    const int L = G.tx >> 2;
     if (loadP) {
-        // rows: warp w loads tile row w and, for w < 2, one halo row (w = 0: below, 1: above)
-        for (int r = w; r < FX_ZM_ROWS; r += 8) {
+        // rows: thread row w loads tile-plus-halo row w and, for w < 2, row w + TY (the
+        // row below the tile is row 0, the row above it row TY + 1)
+        for (int r = G.row; r < G.ty + 2; r += G.ty) {
             const int gy = y0t - 1 + r;
             const int cy = gy < 0 ? 0 : (gy > Y - 1 ? Y - 1 : gy);
-            const PT* row = p + plane + (long long)cy * X;
-            if (x < X) fx_cp4(&sm.p[slot][r][4 + 4 * lane], row + x);
-            if (r >= 1 && r <= FX_ZM_TY) {  // halo segments of the tile rows
-                if (lane == 0 && x0t >= 4) fx_cp4(&sm.p[slot][r][0], row + x0t - 4);
-                if (lane == 31 && x0t + FX_ZM_TX < X) fx_cp4(&sm.p[slot][r][4 + FX_ZM_TX], row + x0t + FX_ZM_TX);
+            const PT* rowp = p + plane + (long long)cy * X;
+            PT* srow = &sm.p[slot][r * G.cols];
+            if (x < X) fx_cp4(srow + 4 + 4 * G.cg, rowp + x);
+            if (r >= 1 && r <= G.ty) {  // halo segments of the tile rows
+                if (G.cg == 0 && x0t >= 4) fx_cp4(srow, rowp + x0t - 4);
+                if (G.cg == L - 1 && x0t + G.tx < X) fx_cp4(srow + 4 + G.tx, rowp + x0t + G.tx);
             }
         }
     }
     if (withDiv) {
-        const int gy = y0t + w;
-        if (x < X && gy < Y) fx_cp_async16(&sm.d[slot][w][4 * lane], div + plane + (long long)gy * X + x);
+        const int gy = y0t + G.row;
+        if (x < X && gy < Y) fx_cp_async16(&sm.d[slot][G.row * G.tx + 4 * G.cg], div + plane + (long long)gy * X + x);
     }
 }
 
@@ -95,16 +128,17 @@ FXD float4 fx_zm_ld4(const __half* p) {
     return make_float4(a.x, a.y, b.x, b.y);
 }
 
-// One z-marching tile of one sweep: planes [z0, z1) of the tile (x0t, y0t). ZERO_IN: the
-// input is known to be zero (the first sweep of a cleared solve): no pressure loads.
-template <typename PT, bool ZERO_IN>
+// One z-marching tile of one sweep: planes [z0, z1) of the tile (x0t, y0t), TX cells wide.
+// ZERO_IN: the input is known to be zero (the first sweep of a cleared solve): no
+// pressure loads.
+template <typename PT, bool ZERO_IN, int TX>
 FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin, PT* __restrict__ pout, int x0t, int y0t,
                     int z0, int z1, FxZmSmem<PT>& sm) {
     const FxSimDev& S = *Sp;
     const int X = S.X, Y = S.Y, Z = S.Z;
     const float* __restrict__ div = S.div;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int x = x0t + 4 * lane, y = y0t + w;
+    const FxZmGeom G = fx_zm_geom<TX>();
+    const int x = x0t + 4 * G.cg, y = y0t + G.row;
     const bool active = x < X && y < Y;
     const FxJacobiConst c{S.jc[0], S.jc[1], S.jc[2], S.jc[3]};
     const float rcpD = S.jcRcp;
@@ -114,15 +148,16 @@ FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin,
     // slot of z-2, refilled with z+4 right after the barrier
     // prologue: planes z0-1 .. z0+3 (pressure), divergence for those in [z0, z1)
     for (int q = z0 - 1; q <= z0 + 3; ++q) {
-        fx_zm_issue<PT>(sm, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, X, Y, Z, x0t, y0t, q, loadP, q >= z0 && q < z1);
+        fx_zm_issue<PT>(sm, G, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, X, Y, Z, x0t, y0t, q, loadP, q >= z0 && q < z1);
         fx_cp_commit();
     }
+    const int r = G.row + 1, col = 4 + 4 * G.cg;
     for (int z = z0; z < z1; ++z) {
         fx_cp_wait<2>();  // this thread's copies of planes up to z + 1 have landed
         __syncthreads();  // ... everyone's; and everyone is done with plane z - 2
         {
             const int q = z + 4;
-            fx_zm_issue<PT>(sm, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, X, Y, Z, x0t, y0t, q, loadP && q <= z1, q < z1);
+            fx_zm_issue<PT>(sm, G, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, X, Y, Z, x0t, y0t, q, loadP && q <= z1, q < z1);
             fx_cp_commit();
         }
         const int sm1 = (z - 1 + FX_ZM_SLOTS) % FX_ZM_SLOTS, s0 = z % FX_ZM_SLOTS, sp1 = (z + 1) % FX_ZM_SLOTS;
@@ -131,18 +166,18 @@ FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin,
             if (y == Y - 1) {
                 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // the open top is the ambient boundary
             } else {
-                const int r = w + 1, col = 4 + 4 * lane;
-                const float4 dv = *reinterpret_cast<const float4*>(&sm.d[s0][w][4 * lane]);
+                const float4 dv = *reinterpret_cast<const float4*>(&sm.d[s0][G.row * G.tx + 4 * G.cg]);
                 float4 cen = make_float4(0, 0, 0, 0), b = cen, t = cen, k = cen, f = cen;
                 float l = 0.0f, rr = 0.0f;
                 if (loadP) {
-                    cen = fx_zm_ld4(&sm.p[s0][r][col]);
-                    b = fx_zm_ld4(&sm.p[s0][r - 1][col]);
-                    t = fx_zm_ld4(&sm.p[s0][r + 1][col]);
-                    k = fx_zm_ld4(&sm.p[sm1][r][col]);
-                    f = fx_zm_ld4(&sm.p[sp1][r][col]);
-                    l = x == 0 ? cen.x : (float)sm.p[s0][r][col - 1];
-                    rr = x + 3 == X - 1 ? cen.w : (float)sm.p[s0][r][col + 4];
+                    const PT* p0 = &sm.p[s0][r * G.cols + col];
+                    cen = fx_zm_ld4(p0);
+                    b = fx_zm_ld4(p0 - G.cols);
+                    t = fx_zm_ld4(p0 + G.cols);
+                    k = fx_zm_ld4(&sm.p[sm1][r * G.cols + col]);
+                    f = fx_zm_ld4(&sm.p[sp1][r * G.cols + col]);
+                    l = x == 0 ? cen.x : (float)p0[-1];
+                    rr = x + 3 == X - 1 ? cen.w : (float)p0[4];
                 }
                 float o[4];
                 o[0] = fx_jacobi_numerator(c, l, cen.y, b.x, t.x, k.x, f.x, dv.x);

@@ -287,16 +287,23 @@ __global__ void __launch_bounds__(FX_ZM_THREADS, 3) fxk_jacobi_zm(const FxBatchD
     fx_for_bricks<FX_SHAPE_ZM>(B, [&](const FxSimDev& S, int b) {
         const int n = phase == 0 ? S.P : S.R;
         if (sweep >= n) return;
-        const int ntx = (S.X + FX_ZM_TX - 1) / FX_ZM_TX, nty = (S.Y + FX_ZM_TY - 1) / FX_ZM_TY;
+        const int TX = fx_zm_tile_w(S.X), TY = FX_ZM_CELLS / TX;
+        const int ntx = (S.X + TX - 1) / TX, nty = (S.Y + TY - 1) / TY;
         const int tx = b % ntx, ty = (b / ntx) % nty, zci = b / (ntx * nty);
         const int z0 = zci * zc, z1 = min(S.Z, z0 + zc);
         const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
-        if (bufs.zeroIn)
-            fx_zm_tile<PT, true>(&S, reinterpret_cast<const PT*>(bufs.pin), reinterpret_cast<PT*>(bufs.pout),
-                                 tx * FX_ZM_TX, ty * FX_ZM_TY, z0, z1, sm);
-        else
-            fx_zm_tile<PT, false>(&S, reinterpret_cast<const PT*>(bufs.pin), reinterpret_cast<PT*>(bufs.pout),
-                                  tx * FX_ZM_TX, ty * FX_ZM_TY, z0, z1, sm);
+        const PT* pin = reinterpret_cast<const PT*>(bufs.pin);
+        PT* pout = reinterpret_cast<PT*>(bufs.pout);
+        const int x0 = tx * TX, y0 = ty * TY;
+        if (bufs.zeroIn) {
+            if (TX == 128) fx_zm_tile<PT, true, 128>(&S, pin, pout, x0, y0, z0, z1, sm);
+            else if (TX == 64) fx_zm_tile<PT, true, 64>(&S, pin, pout, x0, y0, z0, z1, sm);
+            else fx_zm_tile<PT, true, 32>(&S, pin, pout, x0, y0, z0, z1, sm);
+        } else {
+            if (TX == 128) fx_zm_tile<PT, false, 128>(&S, pin, pout, x0, y0, z0, z1, sm);
+            else if (TX == 64) fx_zm_tile<PT, false, 64>(&S, pin, pout, x0, y0, z0, z1, sm);
+            else fx_zm_tile<PT, false, 32>(&S, pin, pout, x0, y0, z0, z1, sm);
+        }
     });
 }
 
