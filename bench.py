@@ -197,30 +197,15 @@ def percentile(xs, q):
 def run_gpu(args) -> None:
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     from fire_b200.sim import FireXSim, make_options
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    else:
-        torch.cuda.set_device(0)
+    from fire_b200.replicas import Replicas
+
+    reps = Replicas("nccl")
+    world, rank = reps.world, reps.rank
     dev = torch.cuda.current_device()
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = reps.barrier, reps.max
 
     sim = FireXSim(DIMS, options(make_options))
     stream = torch.cuda.ExternalStream(sim.stream)
@@ -309,8 +294,7 @@ def run_gpu(args) -> None:
         }
         print(json.dumps(line), flush=True)
     sim.close()
-    if world > 1:
-        dist.destroy_process_group()
+    reps.close()
 
 
 # ---- batched mixed precision: 48 uneven simulations stepped by shared launches --------------

@@ -140,9 +140,7 @@ FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin,
     const FxZmGeom G = fx_zm_geom<TX>();
     const int x = x0t + 4 * G.cg, y = y0t + G.row;
     const bool active = x < X && y < Y;
-    const FxJacobiConst c{S.jc[0], S.jc[1], S.jc[2], S.jc[3]};
-    const float rcpD = S.jcRcp;
-    const bool fastDiv = S.jcFastDiv != 0;
+    const FxJacobiConst2 c2 = fx_jacobi_const2(FxJacobiConst{S.jc[0], S.jc[1], S.jc[2], S.jc[3]}, S.jcRcp, S.jcFastDiv != 0);
     constexpr bool loadP = !ZERO_IN;
     // ring: at plane z, slots hold z-1, z, z+1 (read), z+2, z+3 (in flight) and the
     // slot of z-2, refilled with z+4 right after the barrier
@@ -179,14 +177,7 @@ FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin,
                     l = x == 0 ? cen.x : (float)p0[-1];
                     rr = x + 3 == X - 1 ? cen.w : (float)p0[4];
                 }
-                float o[4];
-                o[0] = fx_jacobi_numerator(c, l, cen.y, b.x, t.x, k.x, f.x, dv.x);
-                o[1] = fx_jacobi_numerator(c, cen.x, cen.z, b.y, t.y, k.y, f.y, dv.y);
-                o[2] = fx_jacobi_numerator(c, cen.y, cen.w, b.z, t.z, k.z, f.z, dv.z);
-                o[3] = fx_jacobi_numerator(c, cen.z, rr, b.w, t.w, k.w, f.w, dv.w);
-#pragma unroll
-                for (int i = 0; i < 4; ++i) o[i] = fastDiv ? fx_div_by_const(o[i], c.denom, rcpD) : __fdiv_rn(o[i], c.denom);
-                out = make_float4(o[0], o[1], o[2], o[3]);
+                out = fx_jacobi4(c2, l, cen, rr, b, t, k, f, dv);
             }
             PStore<PT>::st4(pout, (long long)z * X * Y + (long long)y * X + x, out);
         }

@@ -201,16 +201,7 @@ __global__ void __launch_bounds__(256) fxk_jacobi(const FxBatchDev* __restrict__
             const float4 pt = PStore<PT>::ld4(pin, rowT + r.x0);
             const float4 pk = PStore<PT>::ld4(pin, rowK + r.x0);
             const float4 pf = PStore<PT>::ld4(pin, rowF + r.x0);
-            o.x = fx_jacobi_numerator(c, pl, pc.y, pb.x, pt.x, pk.x, pf.x, d.x);
-            o.y = fx_jacobi_numerator(c, pc.x, pc.z, pb.y, pt.y, pk.y, pf.y, d.y);
-            o.z = fx_jacobi_numerator(c, pc.y, pc.w, pb.z, pt.z, pk.z, pf.z, d.z);
-            o.w = fx_jacobi_numerator(c, pc.z, pr, pb.w, pt.w, pk.w, pf.w, d.w);
-            if (S.jcFastDiv) {
-                o = make_float4(fx_div_by_const(o.x, c.denom, S.jcRcp), fx_div_by_const(o.y, c.denom, S.jcRcp),
-                                fx_div_by_const(o.z, c.denom, S.jcRcp), fx_div_by_const(o.w, c.denom, S.jcRcp));
-            } else {
-                o = make_float4(o.x / c.denom, o.y / c.denom, o.z / c.denom, o.w / c.denom);
-            }
+            o = fx_jacobi4(fx_jacobi_const2(c, S.jcRcp, S.jcFastDiv != 0), pl, pc, pr, pb, pt, pk, pf, d);
         }
         PStore<PT>::st4(pout, row + r.x0, o);
     });
