@@ -88,35 +88,69 @@ FXD FxZmGeom fx_zm_geom() {
     return g;
 }
 
-// Issues the copies of plane q (clamped) into ring slot `slot`: the tile rows, the halo
-// rows and the halo segments (pressure), and the tile rows of the divergence when
-// withDiv (the plane is one the chunk updates).
-template <typename PT>
-FXD void fx_zm_issue(FxZmSmem<PT>& sm, const FxZmGeom& G, int slot, const PT* __restrict__ p, const float* __restrict__ div,
-                     int X, int Y, int Z, int x0t, int y0t, int q, bool loadP, bool withDiv) {
-    const int qc = q < 0 ? 0 : (q > Z - 1 ? Z - 1 : q);
-    const long long plane = (long long)qc * X * Y;
+// This thread's share of the copies of one plane, fixed for the whole tile: offsets
+// within a plane (global) and within a ring slot (shared); -1 marks a copy it does not
+// make. Row r of a slot is tile-plus-halo row r (row 0 below the tile, row TY + 1 above,
+// both clamped into the grid); thread row w copies row w and, for w < 2, row w + TY; the
+// first and last cell groups of a row also copy its 4-cell halo segments.
+struct FxZmPlan {
+    int gP[2], sP[2];   // pressure row segments
+    int gL, sL, gR, sR; // halo segments
+    int gD, sD;         // divergence
+};
+FXD FxZmPlan fx_zm_plan(const FxZmGeom& G, int X, int Y, int x0t, int y0t) {
+    FxZmPlan P;
     const int x = x0t + 4 * G.cg;
     const int L = G.tx >> 2;
-    if (loadP) {
-        // rows: thread row w loads tile-plus-halo row w and, for w < 2, row w + TY (the
-        // row below the tile is row 0, the row above it row TY + 1)
-        for (int r = G.row; r < G.ty + 2; r += G.ty) {
+    P.gL = P.sL = P.gR = P.sR = -1;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int r = G.row + k * G.ty;
+        P.gP[k] = P.sP[k] = -1;
+        if (r < G.ty + 2) {
             const int gy = y0t - 1 + r;
             const int cy = gy < 0 ? 0 : (gy > Y - 1 ? Y - 1 : gy);
-            const PT* rowp = p + plane + (long long)cy * X;
-            PT* srow = &sm.p[slot][r * G.cols];
-            if (x < X) fx_cp4(srow + 4 + 4 * G.cg, rowp + x);
-            if (r >= 1 && r <= G.ty) {  // halo segments of the tile rows
-                if (G.cg == 0 && x0t >= 4) fx_cp4(srow, rowp + x0t - 4);
-                if (G.cg == L - 1 && x0t + G.tx < X) fx_cp4(srow + 4 + G.tx, rowp + x0t + G.tx);
+            if (x < X) {
+                P.gP[k] = cy * X + x;
+                P.sP[k] = r * G.cols + 4 + 4 * G.cg;
+            }
+            if (r >= 1 && r <= G.ty) {
+                if (G.cg == 0 && x0t >= 4) {
+                    P.gL = cy * X + x0t - 4;
+                    P.sL = r * G.cols;
+                }
+                if (G.cg == L - 1 && x0t + G.tx < X) {
+                    P.gR = cy * X + x0t + G.tx;
+                    P.sR = r * G.cols + 4 + G.tx;
+                }
             }
         }
     }
-    if (withDiv) {
-        const int gy = y0t + G.row;
-        if (x < X && gy < Y) fx_cp_async16(&sm.d[slot][G.row * G.tx + 4 * G.cg], div + plane + (long long)gy * X + x);
+    const int gy = y0t + G.row;
+    P.gD = P.sD = -1;
+    if (x < X && gy < Y) {
+        P.gD = gy * X + x;
+        P.sD = G.row * G.tx + 4 * G.cg;
     }
+    return P;
+}
+
+// Issues this thread's copies of plane q (clamped into the grid) into ring slot `slot`:
+// pressure when loadP, divergence when withDiv (the plane is one the chunk updates).
+template <typename PT>
+FXD void fx_zm_issue(FxZmSmem<PT>& sm, const FxZmPlan& P, int slot, const PT* __restrict__ p, const float* __restrict__ div,
+                     long long XY, int Z, int q, bool loadP, bool withDiv) {
+    const int qc = q < 0 ? 0 : (q > Z - 1 ? Z - 1 : q);
+    const long long plane = (long long)qc * XY;
+    if (loadP) {
+        const PT* pp = p + plane;
+        PT* sp = sm.p[slot];
+        if (P.sP[0] >= 0) fx_cp4(sp + P.sP[0], pp + P.gP[0]);
+        if (P.sP[1] >= 0) fx_cp4(sp + P.sP[1], pp + P.gP[1]);
+        if (P.sL >= 0) fx_cp4(sp + P.sL, pp + P.gL);
+        if (P.sR >= 0) fx_cp4(sp + P.sR, pp + P.gR);
+    }
+    if (withDiv && P.sD >= 0) fx_cp_async16(&sm.d[slot][P.sD], div + plane + P.gD);
 }
 
 // Four consecutive shared-memory pressure elements as float4 (one 16- or 8-byte read).
@@ -142,11 +176,13 @@ FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin,
     const bool active = x < X && y < Y;
     const FxJacobiConst2 c2 = fx_jacobi_const2(FxJacobiConst{S.jc[0], S.jc[1], S.jc[2], S.jc[3]}, S.jcRcp, S.jcFastDiv != 0);
     constexpr bool loadP = !ZERO_IN;
+    const FxZmPlan plan = fx_zm_plan(G, X, Y, x0t, y0t);
+    const long long XY = (long long)X * Y;
     // ring: at plane z, slots hold z-1, z, z+1 (read), z+2, z+3 (in flight) and the
     // slot of z-2, refilled with z+4 right after the barrier
     // prologue: planes z0-1 .. z0+3 (pressure), divergence for those in [z0, z1)
     for (int q = z0 - 1; q <= z0 + 3; ++q) {
-        fx_zm_issue<PT>(sm, G, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, X, Y, Z, x0t, y0t, q, loadP, q >= z0 && q < z1);
+        fx_zm_issue<PT>(sm, plan, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, XY, Z, q, loadP, q >= z0 && q < z1);
         fx_cp_commit();
     }
     const int r = G.row + 1, col = 4 + 4 * G.cg;
@@ -155,7 +191,7 @@ FXD void fx_zm_tile(const FxSimDev* __restrict__ Sp, const PT* __restrict__ pin,
         __syncthreads();  // ... everyone's; and everyone is done with plane z - 2
         {
             const int q = z + 4;
-            fx_zm_issue<PT>(sm, G, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, X, Y, Z, x0t, y0t, q, loadP && q <= z1, q < z1);
+            fx_zm_issue<PT>(sm, plan, (q + FX_ZM_SLOTS) % FX_ZM_SLOTS, pin, div, XY, Z, q, loadP && q <= z1, q < z1);
             fx_cp_commit();
         }
         const int sm1 = (z - 1 + FX_ZM_SLOTS) % FX_ZM_SLOTS, s0 = z % FX_ZM_SLOTS, sp1 = (z + 1) % FX_ZM_SLOTS;

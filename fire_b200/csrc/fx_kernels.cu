@@ -134,31 +134,88 @@ FXD Row4 fx_row4(const FxSimDev& S, int b) {
     return r;
 }
 
+// Cells of a ROW4 brick taken lane by lane: the brick's 1024 consecutive cells (memory
+// order) are split per warp into 128, and lane l of a warp takes cells l, l+32, l+64,
+// l+96 of its 128, so every warp-wide load of a float4 record reads 512 contiguous bytes.
+struct Lane4 {
+    int c0;       // first cell (memory index) of this lane
+    int x, y, z;  // its coordinates
+    int n;        // cells of the warp's 128 that exist (the last brick may end early)
+};
+FXD Lane4 fx_lane4(const FxSimDev& S, int b) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int N = S.X * S.Y * S.Z;  // < 2^31
+    const int base = b * (FX_ROW4_THREADS * 4) + w * 128;
+    Lane4 r;
+    r.c0 = base + lane;
+    const int t = r.c0 / S.X;
+    r.x = r.c0 - t * S.X;
+    r.z = t / S.Y;
+    r.y = t - r.z * S.Y;
+    r.n = min(128, max(0, N - base));
+    return r;
+}
+// Coordinates of the lane's four cells (32 apart in memory order).
+FXD void fx_lane4_coords(const FxSimDev& S, const Lane4& r, int xs[4], int ys[4], int zs[4]) {
+    int x = r.x, y = r.y, z = r.z;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        xs[i] = x;
+        ys[i] = y;
+        zs[i] = z;
+        x += 32;
+        while (x >= S.X) {
+            x -= S.X;
+            if (++y == S.Y) {
+                y = 0;
+                ++z;
+            }
+        }
+    }
+}
+
 // ---- computeDivergence (shaders.ts:344-364) ---------------------------------------------
 // phase 0: the predicted flow after simulate; phase 1: the primary-projected flow (the
-// residual solve's right-hand side).
+// residual solve's right-hand side). Backward differences with the clamped neighbour
+// (the cell itself on the low walls). Every load of the lane's four cells is issued
+// before the arithmetic; the x-1 neighbour comes from the next lower lane.
 __global__ void __launch_bounds__(256) fxk_divergence(const FxBatchDev* __restrict__ B, int phase) {
     fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
-        const Row4 r = fx_row4(S, b);
-        if (!r.ok) return;
-        const void* flow = phase == 0 ? S.flow[S.fi ^ 1] : S.flow[S.fi];
+        const Lane4 r = fx_lane4(S, b);
+        if (r.n <= 0) return;  // warp-uniform
+        const int lane = threadIdx.x & 31;
+        const float4* __restrict__ flow = reinterpret_cast<const float4*>(phase == 0 ? S.flow[S.fi ^ 1] : S.flow[S.fi]);
         const float3 m = fx_metric(S.prm.u);
-        const long long X = S.X, XY = (long long)S.X * S.Y;
-        const long long row = (long long)r.y * X + r.z * XY;
-        const long long rowB = (long long)(r.y > 0 ? r.y - 1 : 0) * X + r.z * XY;
-        const long long rowK = (long long)r.y * X + (long long)(r.z > 0 ? r.z - 1 : 0) * XY;
-        float left = fx_ld_flow(flow, row + (r.x0 > 0 ? r.x0 - 1 : 0)).x;
-        float d[4];
+        const int X = S.X, XY = S.X * S.Y;
+        int xs[4], ys[4], zs[4];
+        fx_lane4_coords(S, r, xs, ys, zs);
+        float4 cv[4];
+        float bottom[4], back[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const float4 c = fx_ld_flow(flow, row + r.x0 + i);
-            const float bottom = fx_ld_flow(flow, rowB + r.x0 + i).y;
-            const float back = fx_ld_flow(flow, rowK + r.x0 + i).z;
-            const float l = (i == 0 && r.x0 == 0) ? c.x : left;
-            d[i] = (c.x - l) * m.x + (c.y - bottom) * m.y + (c.z - back) * m.z;
-            left = c.x;
+            const int c = r.c0 + 32 * i;
+            cv[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            bottom[i] = back[i] = 0.0f;
+            if (lane + 32 * i < r.n) {
+                cv[i] = __ldg(flow + c);
+                if (ys[i] > 0) bottom[i] = __ldg(flow + c - X).y;
+                if (zs[i] > 0) back[i] = __ldg(flow + c - XY).z;
+            }
         }
-        *reinterpret_cast<float4*>(S.div + row + r.x0) = make_float4(d[0], d[1], d[2], d[3]);
+        // .x of the cell before lane 0's first cell (a previous warp's or brick's cell)
+        float prevX = (lane == 0 && xs[0] > 0) ? __ldg(flow + r.c0 - 1).x : 0.0f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int c = r.c0 + 32 * i;
+            const float fromLeft = __shfl_up_sync(0xffffffffu, cv[i].x, 1);
+            const float l = xs[i] == 0 ? cv[i].x : (lane > 0 ? fromLeft : prevX);
+            prevX = __shfl_sync(0xffffffffu, cv[i].x, 31);
+            if (lane + 32 * i < r.n) {
+                const float bo = ys[i] > 0 ? bottom[i] : cv[i].y;
+                const float ba = zs[i] > 0 ? back[i] : cv[i].z;
+                S.div[c] = (cv[i].x - l) * m.x + (cv[i].y - bo) * m.y + (cv[i].z - ba) * m.z;
+            }
+        }
     });
 }
 
@@ -216,55 +273,53 @@ __global__ void __launch_bounds__(256) fxk_jacobi(const FxBatchDev* __restrict__
 template <typename PT>
 __global__ void __launch_bounds__(256) fxk_project(const FxBatchDev* __restrict__ B, int phase) {
     fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
-        const Row4 r = fx_row4(S, b);
-        if (!r.ok) return;
-        const void* flowIn;
-        void* flowOut;
+        const Lane4 r = fx_lane4(S, b);
+        if (r.n <= 0) return;
+        const int lane = threadIdx.x & 31;
+        const float4* __restrict__ flowIn;
+        float4* __restrict__ flowOut;
         const void* p;
         bool zeroP;
         if (phase == 0) {
-            flowIn = S.flow[S.fi ^ 1];
-            flowOut = S.flow[S.fi];
+            flowIn = reinterpret_cast<const float4*>(S.flow[S.fi ^ 1]);
+            flowOut = reinterpret_cast<float4*>(S.flow[S.fi]);
             const int base = (S.mode == FIREX_PRESSURE_COLD_F32) ? 0 : S.pi;
             p = S.p[(base + S.P) & 1];
             zeroP = S.mode == FIREX_PRESSURE_COLD_F32 && S.P == 0;
         } else {
-            flowIn = S.flow[S.fi];
-            flowOut = S.flow[S.fi ^ 1];
+            flowIn = reinterpret_cast<const float4*>(S.flow[S.fi]);
+            flowOut = reinterpret_cast<float4*>(S.flow[S.fi ^ 1]);
             p = S.corr[S.R & 1];
             zeroP = S.R == 0;
         }
         const float3 m = fx_metric(S.prm.u);
-        const long long X = S.X, XY = (long long)S.X * S.Y;
-        const int ys = (r.y == S.Y - 1) ? r.y - 1 : r.y;  // top row: the projected row below
-        const long long row = (long long)r.y * X + r.z * XY;
-        const long long rowS = (long long)ys * X + r.z * XY;
-        float4 pc = make_float4(0, 0, 0, 0), pt = pc, pf = pc;
-        float pr = 0.0f;
-        if (!zeroP) {
-            pc = PStore<PT>::ld4(p, rowS + r.x0);
-            pr = r.x0 + 4 < S.X ? PStore<PT>::ld(p, rowS + r.x0 + 4) : pc.w;
-            pt = PStore<PT>::ld4(p, rowS + X + r.x0);  // ys + 1 <= Y - 1 always
-            pf = PStore<PT>::ld4(p, rowS + (r.z < S.Z - 1 ? XY : 0) + r.x0);
-        }
-        const float pcv[4] = {pc.x, pc.y, pc.z, pc.w};
-        const float pxv[4] = {pc.y, pc.z, pc.w, pr};
-        const float ptv[4] = {pt.x, pt.y, pt.z, pt.w};
-        const float pfv[4] = {pf.x, pf.y, pf.z, pf.w};
+        const int X = S.X, XY = S.X * S.Y;
+        int xs[4], ys[4], zs[4];
+        fx_lane4_coords(S, r, xs, ys, zs);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const int x = r.x0 + i;
-            const float4 f = fx_ld_flow(flowIn, row + x);
-            const float4 src = (ys == r.y) ? f : fx_ld_flow(flowIn, rowS + x);
-            const float gx = (pxv[i] - pcv[i]) * m.x;
-            const float gy = (ptv[i] - pcv[i]) * m.y;
-            const float gz = (pfv[i] - pcv[i]) * m.z;
-            float4 o = make_float4(src.x - gx, src.y - gy, src.z - gz, f.w);
-            if (x == 0 || x == S.X - 1) o.x = 0.0f;
-            if (r.z == 0 || r.z == S.Z - 1) o.z = 0.0f;
-            if (r.y == 0) o.y = 0.0f;
-            if (r.y == S.Y - 1) o.y = fx_max(0.0f, o.y);
-            fx_st_flow(flowOut, row + x, o);
+            if (lane + 32 * i < r.n) {
+                const int c = r.c0 + 32 * i;
+                const int cs = (ys[i] == S.Y - 1) ? c - X : c;  // top row: the projected row below
+                const float4 f = __ldg(flowIn + c);
+                const float4 src = (cs == c) ? f : __ldg(flowIn + cs);
+                float pc = 0.0f, px = 0.0f, pt = 0.0f, pf = 0.0f;
+                if (!zeroP) {
+                    pc = PStore<PT>::ld(p, cs);
+                    px = xs[i] + 1 < X ? PStore<PT>::ld(p, cs + 1) : pc;
+                    pt = PStore<PT>::ld(p, cs + X);  // the row above the source row is in the grid
+                    pf = zs[i] < S.Z - 1 ? PStore<PT>::ld(p, cs + XY) : pc;
+                }
+                const float gx = (px - pc) * m.x;
+                const float gy = (pt - pc) * m.y;
+                const float gz = (pf - pc) * m.z;
+                float4 o = make_float4(src.x - gx, src.y - gy, src.z - gz, f.w);
+                if (xs[i] == 0 || xs[i] == X - 1) o.x = 0.0f;
+                if (zs[i] == 0 || zs[i] == S.Z - 1) o.z = 0.0f;
+                if (ys[i] == 0) o.y = 0.0f;
+                if (ys[i] == S.Y - 1) o.y = fx_max(0.0f, o.y);
+                flowOut[c] = o;
+            }
         }
     });
 }

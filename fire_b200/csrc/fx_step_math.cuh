@@ -397,7 +397,12 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     }
     // radiation and decay (shaders.ts:299-304)
     float persistence = fx_clamp(u[U_PERSISTENCE], FC(0.4), 3.0f);
-    float radiation = fx_divc(FC(5.67e-8) * (__ldg(tab + TU_TAMB4) - powf(fx_max(flow.w, 0.0f), 4.0f)), dc[DIVC_RADIATION]);
+    // pow(T, 4): cells at exactly the ambient temperature (every cold cell clamped to it
+    // above) take the per-step table value, which is the same powf of the same input
+    const float tRad = fx_max(flow.w, 0.0f);
+    const float tamb4 = __ldg(tab + TU_TAMB4);
+    const float t4 = tRad == u[U_T_AMBIENT] ? tamb4 : powf(tRad, 4.0f);
+    float radiation = fx_divc(FC(5.67e-8) * (tamb4 - t4), dc[DIVC_RADIATION]);
     flow.w = fx_max(u[U_T_AMBIENT], flow.w + dt * radiation);
     species.z *= __ldg(tab + TU_DECAY_Z);
     species.w *= __ldg(tab + TU_DECAY_W);
