@@ -47,15 +47,16 @@ JACOBI_BYTES_PER_CELL = 12  # read p + read div + write p, f32 (algorithmic, per
 L2_BYTES = 126 * 1024 * 1024
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of the default
-# Jacobi kernel on this workload, from one ncu capture (profiles/jacobi_unblocked_hd.md).
-JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each Jacobi
+# kernel on this workload, from one ncu capture each (profiles/jacobi_*_hd.md).
+JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25234176 + 1516544}
+
+JACOBI_KERNEL_NAMES = {1: "fxk_jacobi<float>", 2: "fxk_jacobi_zm<float>", 3: "fxk_jacobi_tb<float>",
+                       4: "fxk_jacobi_res<float>"}
 
 
 def jacobi_kernel_name(diag: dict) -> str:
-    if diag.get("jacobi_block", 1) > 1:
-        return "fxk_jacobi_tb<K=%d>" % diag["jacobi_block"]
-    return "fxk_jacobi_zm<float>" if diag.get("jacobi_zchunk", 0) > 0 else "fxk_jacobi<float>"
+    return JACOBI_KERNEL_NAMES.get(diag.get("jacobi_kernel"), "fxk_jacobi<float>")
 
 
 def cells() -> int:
@@ -264,8 +265,11 @@ def run_gpu(args) -> None:
     # ---- roofline of the dominant kernel ----
     jac_ms, jac_n = passes["jacobi"]
     jac_avg_ms = jac_ms / max(1, jac_n)
+    # sweeps one launch performs: 1 for single-sweep kernels, a whole phase (P = R sweeps)
+    # for the resident kernel, K for the fused one
+    sweeps_per_launch = (P_ITERS + R_ITERS) * prof_steps / max(1, jac_n)
     peak, peak_kind = measured_peak_hbm()
-    achieved = JACOBI_BYTES_PER_CELL * n_cells / (jac_avg_ms / 1e3) / 1e9
+    achieved = JACOBI_BYTES_PER_CELL * n_cells * sweeps_per_launch / (jac_avg_ms / 1e3) / 1e9
     kernel = jacobi_kernel_name(diag)
     traffic = JACOBI_TRAFFIC_PER_LAUNCH.get(kernel)
 
@@ -285,7 +289,8 @@ def run_gpu(args) -> None:
             "roofline": {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "traffic": traffic, "bytes_per_cell": JACOBI_BYTES_PER_CELL, "avg_launch_us": jac_avg_ms * 1e3,
-                         "launches": jac_n},
+                         "launches": jac_n, "sweeps_per_launch": sweeps_per_launch,
+                         "algorithmic_bytes_per_launch": JACOBI_BYTES_PER_CELL * n_cells * sweeps_per_launch},
             "passes_ms_per_step": {k: v[0] / prof_steps for k, v in passes.items()},
             "profiled_steps": prof_steps,
             "gpu_launches": int(launches),
