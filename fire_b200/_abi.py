@@ -152,6 +152,7 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_read_field": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_write_field": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_divergence_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
+        "firex_read_field_async": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_divergence_norm_noalloc": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float), vp,
                                                     C.POINTER(C.c_double)]),
         "firex_get_state": (C.c_int, [vp, C.POINTER(State)]),
@@ -188,7 +189,7 @@ def declare_firex(lib: C.CDLL) -> None:
 HEADER_SYMBOLS = [
     "firex_default_options", "firex_field_element_size", "firex_create", "firex_destroy",
     "firex_last_error", "firex_set_parameter", "firex_get_parameter", "firex_reset", "firex_step",
-    "firex_sync", "firex_read_field", "firex_write_field", "firex_divergence_norm",
+    "firex_sync", "firex_read_field", "firex_read_field_async", "firex_write_field", "firex_divergence_norm",
     "firex_divergence_norm_noalloc", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_stream", "firex_set_profiling", "firex_pass_times",

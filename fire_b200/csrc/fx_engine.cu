@@ -339,6 +339,13 @@ struct firex_sim {
     void* d_tmp = nullptr;          // 4 B/cell scratch: emitter mask, final divergence
     double* d_partial = nullptr;    // divergence-norm partials
     double* d_norm = nullptr;
+    // overlapped readback (firex_read_field_async): the field is copied on the device into
+    // a staging buffer in stream order, then to the host on a copy stream while later
+    // steps run; created on first use
+    void* d_stage = nullptr;
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t evStaged = nullptr, evCopied = nullptr;
+    bool copyPending = false;
     std::string err;
     bool poisoned = false;
 
@@ -825,6 +832,16 @@ void firex_sim::release() {
         solo = nullptr;
     }
     if (own) cudaStreamSynchronize(own);
+    if (copyStream) {
+        cudaStreamSynchronize(copyStream);
+        cudaStreamDestroy(copyStream);
+        copyStream = nullptr;
+    }
+    if (evStaged) cudaEventDestroy(evStaged);
+    if (evCopied) cudaEventDestroy(evCopied);
+    evStaged = evCopied = nullptr;
+    copyPending = false;
+    d_stage = nullptr;
     for (void* p : allocations) cudaFree(p);
     allocations.clear();
     if (own) cudaStreamDestroy(own);
@@ -1059,7 +1076,9 @@ int firex_sync(firex_sim* s) {
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
     DeviceGuard dg(s->device);
     cudaError_t e = cudaStreamSynchronize(s->stream());
+    if (e == cudaSuccess && s->copyStream) e = cudaStreamSynchronize(s->copyStream);
     if (e != cudaSuccess) return s->cuda_fail(e, "sync");
+    s->copyPending = false;
     return s->check_device_waits();
 }
 
@@ -1116,6 +1135,39 @@ int firex_read_field(firex_sim* s, int32_t field, void* host, size_t bytes) {
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return s->cuda_fail(e, "read_field");
+    return FIREX_OK;
+}
+
+int firex_read_field_async(firex_sim* s, int32_t field, void* host, size_t bytes) {
+    if (!s || !host) return FIREX_ERR_BAD_ARG;
+    if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
+    const size_t es = firex_field_element_size(field);
+    if (!es) return s->fail(FIREX_ERR_BAD_ARG, "unknown field id");
+    if (bytes != es * (size_t)s->N) return s->fail(FIREX_ERR_BAD_ARG, "byte count does not match the field size");
+    const bool direct = field == FIREX_FIELD_FLOW || field == FIREX_FIELD_DIVERGENCE || field == FIREX_FIELD_REACTION ||
+                        field == FIREX_FIELD_LIQUID || (field == FIREX_FIELD_SPECIES && s->storage == FX_STORAGE_F32) ||
+                        (field == FIREX_FIELD_PRESSURE && !s->half && s->mode != FIREX_PRESSURE_COLD_F32) ||
+                        (field == FIREX_FIELD_CORRECTION && !s->half && s->h.R > 0);
+    if (!direct) return s->fail(FIREX_ERR_UNSUPPORTED, "this field needs a host-side conversion: use firex_read_field");
+    DeviceGuard dg(s->device);
+    cudaError_t e = cudaSuccess;
+    if (!s->copyStream) {
+        e = cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->evStaged, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->evCopied, cudaEventDisableTiming);
+        if (e == cudaSuccess && !(s->d_stage = s->alloc((size_t)s->N * 16))) e = cudaErrorMemoryAllocation;
+        if (e != cudaSuccess) return s->cuda_fail(e, "read_field_async set-up");
+    }
+    cudaStream_t st = s->stream();
+    // the staging buffer is free once the previous host copy has finished
+    if (s->copyPending) e = cudaStreamWaitEvent(st, s->evCopied, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_stage, field_buffer(s, field), bytes, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaEventRecord(s->evStaged, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s->copyStream, s->evStaged, 0);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host, s->d_stage, bytes, cudaMemcpyDeviceToHost, s->copyStream);
+    if (e == cudaSuccess) e = cudaEventRecord(s->evCopied, s->copyStream);
+    if (e != cudaSuccess) return s->cuda_fail(e, "read_field_async");
+    s->copyPending = true;
     return FIREX_OK;
 }
 
@@ -1377,6 +1429,11 @@ int firex_batch_sync(firex_batch* b) {
     cudaError_t e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return b->poison(e, "batch sync");
     for (firex_sim* s : b->members) {
+        if (s->copyStream) {
+            e = cudaStreamSynchronize(s->copyStream);
+            if (e != cudaSuccess) return b->poison(e, "batch sync (readback)");
+            s->copyPending = false;
+        }
         const int rc = s->check_device_waits();
         if (rc != FIREX_OK) return b->fail(rc, s->err);
     }

@@ -228,6 +228,13 @@ class FireXSim(_Handle):
     def __init__(self, dims: Iterable[int], options: A.Options | None = None, **kw):
         super().__init__(load_library(), dims, options, **kw)
 
+    def read_async(self, field, out: np.ndarray) -> np.ndarray:
+        """Starts an overlapped copy of `field` (as it stands after the steps enqueued so
+        far) into `out`; `out` is complete after sync(). Use pinned memory for overlap."""
+        f = A.FIELD_NAMES[field] if isinstance(field, str) else int(field)
+        self._check(self._lib.firex_read_field_async(self._h, f, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
     @property
     def device_bytes(self) -> int:
         v = C.c_uint64()

@@ -166,6 +166,17 @@ int firex_sync(firex_sim* sim);
 int firex_read_field(firex_sim* sim, int32_t field, void* host, size_t bytes);
 int firex_write_field(firex_sim* sim, int32_t field, const void* host, size_t bytes);
 
+/* Overlapped readback of a field (no reference counterpart: the reference reads no field
+ * back). The field as it stands after the steps enqueued so far is copied in stream order
+ * into a device staging buffer, then to `host` on a separate copy stream, so the copy
+ * overlaps the steps enqueued after this call. `host` must stay valid (and should be
+ * pinned, or the copy does not overlap) until firex_sync (or firex_batch_sync); a second
+ * call waits on the device for the first copy to leave the staging buffer. Fields whose
+ * host form needs a conversion (FP16 storage, emitter mask, final divergence) are
+ * refused with FIREX_ERR_UNSUPPORTED: use firex_read_field. The first call allocates the
+ * staging buffer (16 B/cell) and the copy stream. */
+int firex_read_field_async(firex_sim* sim, int32_t field, void* host, size_t bytes);
+
 /* Post-projection divergence of FLOW over interior cells (the one-cell outer shell is
  * excluded, qualityShaders.ts:47-57), reduced in FP64: out[0] = L2 norm, out[1] = max
  * abs, out[2] = number of interior cells. (Presentation diagnostic, FireXEngine.ts:2588-2596.) */
