@@ -130,10 +130,11 @@ struct StepPlan {
     bool row4 = false;        // single sweeps by the unblocked kernel instead
     bool fuseP = false, fuseR = false;
     bool res = false;         // every sweep of a phase in one resident launch
+    int resVariant = 0;       // ... by this variant of the kernel
     int resSmem = 0;          // its dynamic shared memory per CTA
     int bricks[FX_NSHAPES] = {};
     auto key() const {
-        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, res, resSmem, bricks[0],
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, res, resVariant, resSmem, bricks[0],
                         bricks[1], bricks[2], bricks[3], bricks[4], bricks[5]);
     }
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
@@ -154,7 +155,7 @@ int jacobi_phase_launches(const StepPlan& pl, int phase) {
 void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, int phase) {
     const int n = phase == 0 ? pl.maxP : pl.maxR;
     if (pl.res) {  // a failed launch is reported by the caller's cudaGetLastError
-        if (n > 0) fx_launch_jacobi_res(st, pl.half, B, pl.bricks[FX_SHAPE_RES], phase, pl.resSmem);
+        if (n > 0) fx_launch_jacobi_res(st, pl.half, pl.resVariant, B, pl.bricks[FX_SHAPE_RES], phase, pl.resSmem);
         return;
     }
     const bool fuse = phase == 0 ? pl.fuseP : pl.fuseR;
@@ -191,26 +192,42 @@ void default_jacobi(long long cells, int* kernel, int* zc) {
     *zc = 32;
 }
 
-// Box decomposition of an X x Y x Z grid over at most m CTAs for the resident Jacobi.
-// A CTA's threads take the box's (x group, row) columns, each split into parts along z
-// when columns are fewer than threads, so a thread computes zlen = ceil(bz / parts)
-// groups per sweep. Cost per sweep: zlen plus the halo traffic per thread (faces written
-// and halo rows read, 2 (by + bz) rows of X / 4 groups, both ways). False when no box
-// fits one CTA's shared memory and registers.
-bool res_box(int X, int Y, int Z, int m, FxResBox* out) {
-    const int gx = X / 4;
+// Box decomposition of an X x Y x Z grid over at most m CTAs for the resident Jacobi
+// (boxes of by x bz full x rows; G = by * bz * X / 4 groups of 4 cells per box). Cost per
+// sweep: the groups a thread computes plus the halo traffic per thread (faces written and
+// halo rows read, 2 (by + bz) rows of X / 4 groups, both ways).
+//   variants 1, 2 (faces-first): face groups and interior groups dealt out separately,
+//     within FX_RES_MAXF and FX_RES_MAXI (variant 2: FX_RES_MAXI_SMALL) per thread;
+//   variant 0 (columns): thread columns of (x group, row), by * X / 4 <= T, each split into
+//     parts along z; at most FX_RES_MAXG planes per column part.
+// False when no box fits one CTA's shared memory and registers.
+bool res_box(int X, int Y, int Z, int m, int variant, FxResBox* out) {
+    const long long gx = X / 4;
     bool found = false;
     double best = 0;
-    for (int by = 1; by <= Y && (long long)by * gx <= FX_RES_THREADS; ++by) {
+    for (int by = 1; by <= Y && by <= 2047; ++by) {
         const int nby = (Y + by - 1) / by;
         if (nby > m || nby > FX_RES_MAX_CTAS) continue;
         const int maxNbz = m / nby;
         const int bz = (Z + maxNbz - 1) / maxNbz;
+        if (bz > 1023) continue;
         if (fx_res_smem_bytes(X, by, bz) > FX_RES_SMEM_MAX) continue;
-        const int parts = FX_RES_THREADS / (by * gx);
-        const int zlen = (bz + parts - 1) / parts;
-        if (zlen > FX_RES_MAXG) continue;
-        const double cost = zlen + 4.0 * (by + bz) * gx / FX_RES_THREADS;
+        const long long G = (long long)by * bz * gx;
+        double work;
+        if (variant != 0) {
+            // faces (at most 2 (by + bz) rows of groups) and interior dealt out separately
+            const int maxi = variant == 2 ? FX_RES_MAXI_SMALL : FX_RES_MAXI;
+            if (2LL * (by + bz) * gx > (long long)FX_RES_MAXF * FX_RES_THREADS) continue;
+            if (G > (long long)maxi * FX_RES_THREADS) continue;
+            work = (double)((G + FX_RES_THREADS - 1) / FX_RES_THREADS);
+        } else {
+            if (by * gx > FX_RES_THREADS) continue;
+            const int parts = (int)(FX_RES_THREADS / (by * gx));
+            const int zlen = (bz + parts - 1) / parts;
+            if (zlen > FX_RES_MAXG) continue;
+            work = zlen;
+        }
+        const double cost = work + 4.0 * (by + bz) * gx / FX_RES_THREADS;
         if (!found || cost < best) {
             found = true;
             best = cost;
@@ -220,10 +237,11 @@ bool res_box(int X, int Y, int Z, int m, FxResBox* out) {
     return found;
 }
 
-// CTAs for every simulation of a batch within `cap` (one launch): each gets at least the
-// fewest CTAs its grid fits in, the rest in proportion to cells. False when the batch
-// does not fit.
-bool res_assign(const std::vector<std::array<int, 3>>& dims, int cap, std::vector<FxResBox>* boxes, int* smem) {
+// CTAs for every simulation of a batch within `cap` (one launch of one variant): each gets
+// at least the fewest CTAs its grid fits in, the rest in proportion to cells. False when
+// the batch does not fit.
+bool res_assign(const std::vector<std::array<int, 3>>& dims, int cap, int variant, std::vector<FxResBox>* boxes,
+                int* smem) {
     const size_t n = dims.size();
     if (n == 0 || cap <= 0) return false;
     std::vector<int> mins(n), t(n);
@@ -232,11 +250,11 @@ bool res_assign(const std::vector<std::array<int, 3>>& dims, int cap, std::vecto
     FxResBox tmp;
     for (size_t i = 0; i < n; ++i) {
         const auto& d = dims[i];
-        if (!res_box(d[0], d[1], d[2], cap, &tmp)) return false;
+        if (!res_box(d[0], d[1], d[2], cap, variant, &tmp)) return false;
         int lo = 1, hi = cap;
         while (lo < hi) {
             const int mid = (lo + hi) / 2;
-            if (res_box(d[0], d[1], d[2], mid, &tmp)) hi = mid;
+            if (res_box(d[0], d[1], d[2], mid, variant, &tmp)) hi = mid;
             else lo = mid + 1;
         }
         mins[i] = lo;
@@ -260,7 +278,7 @@ bool res_assign(const std::vector<std::array<int, 3>>& dims, int cap, std::vecto
     boxes->resize(n);
     *smem = 0;
     for (size_t i = 0; i < n; ++i) {
-        res_box(dims[i][0], dims[i][1], dims[i][2], t[i], &(*boxes)[i]);
+        res_box(dims[i][0], dims[i][1], dims[i][2], t[i], variant, &(*boxes)[i]);
         *smem = std::max(*smem, (int)fx_res_smem_bytes(dims[i][0], (*boxes)[i].by, (*boxes)[i].bz));
     }
     return true;
@@ -501,6 +519,7 @@ struct firex_batch {
     int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
     int tableRes = -1;                               // whether resident boxes were requested
     bool resOk = false;                              // ... and the batch fits one resident launch
+    int resVariant = 0;                              // ... of this kernel variant
     int resSmem = 0;
     std::string err;
 
@@ -533,7 +552,16 @@ struct firex_batch {
         if (wantRes && !members.empty()) {
             std::vector<std::array<int, 3>> dims;
             for (firex_sim* s : members) dims.push_back({s->X, s->Y, s->Z});
-            resOk = res_assign(dims, fx_res_capacity(members[0]->half), &boxes, &resSmem);
+            // the faces-first variant (its small-box instance first) when every member fits
+            // it, else the column variant
+            const int cap = fx_res_capacity(members[0]->half);
+            for (int v : {2, 1, 0}) {
+                if (res_assign(dims, cap, v, &boxes, &resSmem)) {
+                    resOk = true;
+                    resVariant = v;
+                    break;
+                }
+            }
         }
         for (size_t i = 0; i < members.size(); ++i) {
             firex_sim* s = members[i];
@@ -607,6 +635,7 @@ struct firex_batch {
         p.res = wantRes && resOk;
         if (p.res) {
             p.resSmem = resSmem;
+            p.resVariant = resVariant;
             p.k = 1;
             p.fuseP = p.fuseR = false;
         }

@@ -25,9 +25,12 @@ enum { FX_TB_F32 = 0, FX_TB_F16_ROUND = 1, FX_TB_F16 = 2 };
 bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc);
 void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase);
 // Every sweep of a phase in one cooperative launch of `ctas` CTAs with `smem` bytes of
-// dynamic shared memory (fx_jacobi_res.cuh); fx_res_capacity: the most CTAs one such
-// launch can hold resident on this device (0 when unavailable).
-cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, const FxBatchDev* B, int ctas, int phase, int smem);
+// dynamic shared memory (fx_jacobi_res.cuh; variant 0 column, 1 faces-first, 2 faces-first
+// for small boxes);
+// fx_res_capacity: the most CTAs one such launch can hold resident on this device (0 when
+// unavailable).
+cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, int variant, const FxBatchDev* B, int ctas, int phase,
+                                 int smem);
 int fx_res_capacity(bool half);
 
 // Single-simulation utilities.

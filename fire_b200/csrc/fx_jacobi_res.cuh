@@ -6,11 +6,12 @@
 // one-row halo on each side in y and z, and its divergence in shared memory for the
 // whole phase. A sweep reads only shared memory: each thread computes its groups of 4
 // consecutive x cells into registers, the CTA synchronises, then writes the new values
-// back. Only box faces leave the SM: after every sweep but the last, the cells a
-// neighbour box needs are stored to the sweep's output buffer, the CTA publishes a
-// per-box flag (release store) and waits for the flags of its up to four neighbours
-// (acquire loads, bounded waits), then loads its halo rows from that buffer through L2
-// (ld.global.cg: L1 may hold stale lines). Only neighbours synchronise, so there is no
+// back. Only box faces leave the SM: every sweep but the last computes the face groups
+// first, stores them to the sweep's output buffer and publishes a per-box flag (release
+// store), then computes the interior while the flag travels; after writing the new
+// values back it waits for the flags of its up to four neighbours (acquire loads, bounded
+// waits) and loads its halo rows from that buffer through L2 (ld.global.cg: L1 may hold
+// stale lines). Only neighbours synchronise, so there is no
 // group-wide barrier. A box rewrites a buffer two sweeps later, after its neighbours
 // published the sweep in between, which they do only after reading that buffer's halo.
 //
@@ -32,7 +33,10 @@
 #include "fx_storage.cuh"
 
 #define FX_RES_THREADS 512
-#define FX_RES_MAXG 12                // groups of 4 cells per thread
+#define FX_RES_MAXG 12                // groups of 4 cells per thread, column variant
+#define FX_RES_MAXF 4                 // face groups per thread, faces-first variant
+#define FX_RES_MAXI 11                // interior groups per thread, faces-first variant
+#define FX_RES_MAXI_SMALL 7           // ... its instance for small boxes (fewer registers)
 #define FX_RES_SMEM_MAX (226 * 1024)  // dynamic shared memory per CTA (227 KB opt-in less static)
 #define FX_RES_SPIN_LIMIT (1u << 24)  // polls of a neighbour's flag (well over a second with back-off)
 #define FX_RES_MAX_CTAS 1024          // boxes per simulation and phase (flag slots)
@@ -69,6 +73,27 @@ FXD void fx_st_release_u32(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
+// Waits until each neighbour box has published sweep s (flag >= s + 1: acquire loads, one
+// thread per neighbour, each wait bounded), then synchronises the CTA. False when a wait
+// expired (the error word is then set).
+FXD bool fx_res_wait(const unsigned* flags, const int nb[4], unsigned s, unsigned* err, int* flag) {
+    if (threadIdx.x == 0) *flag = 1;
+    __syncthreads();
+    if (threadIdx.x < 4 && nb[threadIdx.x] >= 0) {
+        unsigned spins = 0;
+        while (fx_ld_acquire_u32(flags + nb[threadIdx.x]) < s + 1) {
+            if (++spins > FX_RES_SPIN_LIMIT) {
+                atomicExch(err, 1u);
+                *flag = 0;
+                break;
+            }
+            if (spins > 64) __nanosleep(32);
+        }
+    }
+    __syncthreads();
+    return *flag != 0;
+}
+
 // Publishes this CTA's faces of sweep s (flag = s + 1, a release store after the CTA
 // barrier, so every thread's face stores are visible first) and waits until each
 // neighbour box has published sweep s (acquire loads, one thread per neighbour, each
@@ -95,46 +120,103 @@ FXD bool fx_res_exchange(unsigned* flags, int me, const int nb[4], unsigned s, u
     return *flag != 0;
 }
 
-// One CTA's share of a resident phase. PT: pressure storage; ROUND: round every sweep's
-// output to FP16 (pressure stored in FP16).
-template <typename PT, bool ROUND>
-FXD void fx_res_box(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
-    __shared__ int s_flag;
-    const int n = phase == 0 ? S.P : S.R;
-    const int X = S.X, Y = S.Y, Z = S.Z;
-    const long long XY = (long long)X * Y;
-    const int iy = b % bx.nby, iz = b / bx.nby;
-    const int y0 = iy * bx.by, z0 = iz * bx.bz;
-    const int ny = min(bx.by, Y - y0), nz = min(bx.bz, Z - z0);
-    const int gx = X >> 2;
-    const int rowsP = bx.by + 2;
-    float* sp = sm;                                            // [(lz+1)*rowsP + ly+1][X]
-    float* sd = sm + (long long)(bx.bz + 2) * rowsP * X;       // [lz*by + ly][X]
-    const bool nbLoY = y0 > 0, nbHiY = y0 + ny < Y, nbLoZ = z0 > 0, nbHiZ = z0 + nz < Z;
-    unsigned* flags = S.sync + FX_RES_FLAGS + phase * FX_RES_MAX_CTAS;
-    unsigned* err = S.sync + 2;
-    // neighbour boxes within the group (-1: none)
-    const int nb[4] = {nbLoY ? b - 1 : -1, nbHiY ? b + 1 : -1, nbLoZ ? b - bx.nby : -1, nbHiZ ? b + bx.nby : -1};
+// Geometry of CTA b's box and its neighbours, and the box's first load.
+struct FxResCtx {
+    int X, Y, Z, n, y0, z0, ny, nz, gx, rowsP;
+    long long XY;
+    float *sp, *sd;  // pressure [(lz+1)*rowsP + ly+1][X] with halo rows; divergence [lz*by + ly][X]
+    bool nbLoY, nbHiY, nbLoZ, nbHiZ;
+    int nb[4];       // neighbour boxes within the group (-1: none)
+    unsigned* flags;
+    unsigned* err;
+};
 
+template <typename PT>
+FXD FxResCtx fx_res_setup(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
+    FxResCtx c;
+    c.n = phase == 0 ? S.P : S.R;
+    c.X = S.X;
+    c.Y = S.Y;
+    c.Z = S.Z;
+    c.XY = (long long)c.X * c.Y;
+    const int iy = b % bx.nby, iz = b / bx.nby;
+    c.y0 = iy * bx.by;
+    c.z0 = iz * bx.bz;
+    c.ny = min(bx.by, c.Y - c.y0);
+    c.nz = min(bx.bz, c.Z - c.z0);
+    c.gx = c.X >> 2;
+    c.rowsP = bx.by + 2;
+    c.sp = sm;
+    c.sd = sm + (long long)(bx.bz + 2) * c.rowsP * c.X;
+    c.nbLoY = c.y0 > 0;
+    c.nbHiY = c.y0 + c.ny < c.Y;
+    c.nbLoZ = c.z0 > 0;
+    c.nbHiZ = c.z0 + c.nz < c.Z;
+    c.nb[0] = c.nbLoY ? b - 1 : -1;
+    c.nb[1] = c.nbHiY ? b + 1 : -1;
+    c.nb[2] = c.nbLoZ ? b - bx.nby : -1;
+    c.nb[3] = c.nbHiZ ? b + bx.nby : -1;
+    c.flags = S.sync + FX_RES_FLAGS + phase * FX_RES_MAX_CTAS;
+    c.err = S.sync + 2;
+    // the box with its halo rows (clamped rows outside the grid are never read) and its divergence
     const FxSolveBufs b0 = fx_solve_bufs(S, phase, 0);
-    // ---- load the box with its halo rows (clamped rows outside the grid are never read)
-    {
-        const int rows = (nz + 2) * (ny + 2);
-        for (int i = threadIdx.x; i < rows * gx; i += blockDim.x) {
-            const int row = i / gx, q = i - row * gx;
-            const int lz = row / (ny + 2) - 1, ly = row % (ny + 2) - 1;
-            const int cz = min(max(z0 + lz, 0), Z - 1), cy = min(max(y0 + ly, 0), Y - 1);
-            float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (!b0.zeroIn) v = PStore<PT>::ld4(b0.pin, cz * XY + (long long)cy * X + 4 * q);
-            *reinterpret_cast<float4*>(sp + ((lz + 1) * rowsP + ly + 1) * X + 4 * q) = v;
-        }
-        for (int i = threadIdx.x; i < nz * ny * gx; i += blockDim.x) {
-            const int row = i / gx, q = i - row * gx;
-            const int lz = row / ny, ly = row - lz * ny;
-            *reinterpret_cast<float4*>(sd + (lz * bx.by + ly) * X + 4 * q) =
-                __ldg(reinterpret_cast<const float4*>(S.div + (z0 + lz) * XY + (long long)(y0 + ly) * X + 4 * q));
-        }
+    const int gx = c.gx, ny = c.ny, nz = c.nz, X = c.X;
+    const int rows = (nz + 2) * (ny + 2);
+    for (int i = threadIdx.x; i < rows * gx; i += blockDim.x) {
+        const int row = i / gx, q = i - row * gx;
+        const int lz = row / (ny + 2) - 1, ly = row % (ny + 2) - 1;
+        const int cz = min(max(c.z0 + lz, 0), c.Z - 1), cy = min(max(c.y0 + ly, 0), c.Y - 1);
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (!b0.zeroIn) v = PStore<PT>::ld4(b0.pin, cz * c.XY + (long long)cy * X + 4 * q);
+        *reinterpret_cast<float4*>(c.sp + ((lz + 1) * c.rowsP + ly + 1) * X + 4 * q) = v;
     }
+    for (int i = threadIdx.x; i < nz * ny * gx; i += blockDim.x) {
+        const int row = i / gx, q = i - row * gx;
+        const int lz = row / ny, ly = row - lz * ny;
+        *reinterpret_cast<float4*>(c.sd + (lz * bx.by + ly) * X + 4 * q) =
+            __ldg(reinterpret_cast<const float4*>(S.div + (c.z0 + lz) * c.XY + (long long)(c.y0 + ly) * X + 4 * q));
+    }
+    return c;
+}
+
+// Halo rows of the next sweep from the neighbours' faces in `pout`, then a CTA barrier.
+template <typename PT>
+FXD void fx_res_halo(const FxResCtx& c, const void* pout) {
+    const int gx = c.gx, ny = c.ny, nz = c.nz, X = c.X;
+    const int hy = (c.nbLoY ? nz : 0) + (c.nbHiY ? nz : 0);
+    const int hz = (c.nbLoZ ? ny : 0) + (c.nbHiZ ? ny : 0);
+    for (int i = threadIdx.x; i < (hy + hz) * gx; i += blockDim.x) {
+        const int row = i / gx, q = i - row * gx;
+        int ly, lz;
+        if (row < hy) {
+            const bool lo = c.nbLoY && row < nz;
+            lz = lo ? row : row - (c.nbLoY ? nz : 0);
+            ly = lo ? -1 : ny;
+        } else {
+            const int r = row - hy;
+            const bool lo = c.nbLoZ && r < ny;
+            ly = lo ? r : r - (c.nbLoZ ? ny : 0);
+            lz = lo ? -1 : nz;
+        }
+        const float4 v = fx_res_ld4_cg<PT>(pout, (c.z0 + lz) * c.XY + (long long)(c.y0 + ly) * X + 4 * q);
+        *reinterpret_cast<float4*>(c.sp + ((lz + 1) * c.rowsP + ly + 1) * X + 4 * q) = v;
+    }
+    __syncthreads();
+}
+
+// Column variant: thread t takes the box's (x group, row) column t and walks its z planes
+// with the z neighbours in registers; the CTA publishes all faces after the whole sweep.
+// For boxes with up to FX_RES_MAXG planes per thread column (the HD tier's 16 x 11 rows).
+template <typename PT, bool ROUND>
+FXD void fx_res_box_col(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
+    __shared__ int s_flag;
+    const FxResCtx cx = fx_res_setup<PT>(S, bx, b, phase, sm);
+    const int n = cx.n, X = cx.X, Y = cx.Y, Z = cx.Z, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, gx = cx.gx;
+    const int rowsP = cx.rowsP;
+    const long long XY = cx.XY;
+    float* sp = cx.sp;
+    const float* sd = cx.sd;
+    const bool nbLoY = cx.nbLoY, nbHiY = cx.nbHiY, nbLoZ = cx.nbLoZ, nbHiZ = cx.nbHiZ;
     // ---- this thread's z column: groups (q, ly, lz) for lz in [zs, zs + cnt). Columns
     // (q, ly) are spread over the threads, each split into P parts along z when there are
     // fewer columns than threads; the planner keeps cnt <= FX_RES_MAXG.
@@ -196,26 +278,165 @@ FXD void fx_res_box(const FxSimDev& S, const FxResBox& bx, int b, int phase, flo
             }
         }
         if (last) break;
-        if (!fx_res_exchange(flags, b, nb, (unsigned)s, err, &s_flag)) return;
-        // ---- halo rows of the next sweep from the neighbours' faces
-        const int hy = (nbLoY ? nz : 0) + (nbHiY ? nz : 0);
-        const int hz = (nbLoZ ? ny : 0) + (nbHiZ ? ny : 0);
-        for (int i = threadIdx.x; i < (hy + hz) * gx; i += blockDim.x) {
-            const int row = i / gx, q = i - row * gx;
-            int ly, lz;
-            if (row < hy) {
-                const bool lo = nbLoY && row < nz;
-                lz = lo ? row : row - (nbLoY ? nz : 0);
-                ly = lo ? -1 : ny;
-            } else {
-                const int r = row - hy;
-                const bool lo = nbLoZ && r < ny;
-                ly = lo ? r : r - (nbLoZ ? ny : 0);
-                lz = lo ? -1 : nz;
-            }
-            const float4 v = fx_res_ld4_cg<PT>(pout, (z0 + lz) * XY + (long long)(y0 + ly) * X + 4 * q);
-            *reinterpret_cast<float4*>(sp + ((lz + 1) * rowsP + ly + 1) * X + 4 * q) = v;
+        if (!fx_res_exchange(cx.flags, b, cx.nb, (unsigned)s, cx.err, &s_flag)) return;
+        fx_res_halo<PT>(cx, pout);
+    }
+}
+
+// Faces-first variant: the face groups are dealt out over all threads and computed
+// first, stored and published before the interior is computed, so the flag travels while
+// the CTA works. For boxes with at most FX_RES_MAXF face groups and FX_RES_MAXI interior
+// groups per thread.
+template <typename PT, bool ROUND, int MAXI>
+FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
+    __shared__ int s_flag;
+    const FxResCtx cx = fx_res_setup<PT>(S, bx, b, phase, sm);
+    const int n = cx.n, X = cx.X, Y = cx.Y, Z = cx.Z, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, gx = cx.gx;
+    const int rowsP = cx.rowsP;
+    const long long XY = cx.XY;
+    float* sp = cx.sp;
+    const float* sd = cx.sd;
+    const bool nbLoY = cx.nbLoY, nbHiY = cx.nbHiY, nbLoZ = cx.nbLoZ, nbHiZ = cx.nbHiZ;
+    // ---- this thread's groups of 4 x cells. The face groups (those a neighbour box reads:
+    // y rows 0 / ny-1 and z planes 0 / nz-1 that have a neighbour) come first, then the
+    // interior ones; each list is dealt out round-robin over the threads, so every thread
+    // holds ceil(F/T) face slots then ceil(I/T) interior slots (the planner keeps their sum
+    // within FX_RES_MAXF and MAXI). Packed as q | ly << 10 | lz << 21, -1 when empty.
+    const int T = blockDim.x, t = threadIdx.x;
+    const int fy0 = nbLoY ? 0 : -1, fy1 = (nbHiY && !(ny == 1 && nbLoY)) ? ny - 1 : -1;
+    const int fz0 = nbLoZ ? 0 : -1, fz1 = (nbHiZ && !(nz == 1 && nbLoZ)) ? nz - 1 : -1;
+    const int nyf = (fy0 >= 0) + (fy1 >= 0), nzf = (fz0 >= 0) + (fz1 >= 0);
+    const int lyA = nbLoY ? 1 : 0, nyi = max(0, (nbHiY ? ny - 1 : ny) - lyA);  // rows off the y faces
+    const int lzA = nbLoZ ? 1 : 0, nzi = max(0, (nbHiZ ? nz - 1 : nz) - lzA);  // planes off the z faces
+    const int FY = nyf * nz * gx, F = FY + nzf * nyi * gx, I = nzi * nyi * gx;
+    int pf[FX_RES_MAXF], pi[MAXI];  // this thread's face / interior groups
+#pragma unroll
+    for (int k = 0; k < FX_RES_MAXF; ++k) {
+        const int i = t + k * T;
+        int q = 0, ly = 0, lz = 0;
+        if (i < FY) {
+            q = i % gx;
+            const int r = i / gx;
+            lz = r % nz;
+            ly = (r / nz == 0 && fy0 >= 0) ? fy0 : fy1;
+        } else if (i < F) {
+            const int j = i - FY;
+            q = j % gx;
+            const int r = j / gx;
+            ly = lyA + r % nyi;
+            lz = (r / nyi == 0 && fz0 >= 0) ? fz0 : fz1;
         }
-        __syncthreads();
+        pf[k] = i < F ? (q | (ly << 10) | (lz << 21)) : -1;
+    }
+#pragma unroll
+    for (int k = 0; k < MAXI; ++k) {
+        const int j = t + k * T;
+        int q = 0, ly = 0, lz = 0;
+        if (j < I) {
+            q = j % gx;
+            const int r = j / gx;
+            ly = lyA + r % nyi;
+            lz = lzA + r / nyi;
+        }
+        pi[k] = j < I ? (q | (ly << 10) | (lz << 21)) : -1;
+    }
+    const FxJacobiConst2 c2 = fx_jacobi_const2(FxJacobiConst{S.jc[0], S.jc[1], S.jc[2], S.jc[3]}, S.jcRcp, S.jcFastDiv != 0);
+    const int planeP = rowsP * X;
+    // The packed coordinates pass through an empty asm on every use, so the compiler
+    // recomputes the offsets each sweep instead of keeping one set per slot live across
+    // the sweep loop (which spills).
+    auto fresh = [](int g) {
+        asm volatile("" : "+r"(g));
+        return g;
+    };
+    // new value of group pk from the old values in shared memory
+    auto update = [&](int g) {
+        const int q = g & 0x3ff, ly = (g >> 10) & 0x7ff, lz = g >> 21;
+        const int y = y0 + ly, z = z0 + lz, x0 = 4 * q;
+        if (y == Y - 1) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // the open top is the ambient boundary
+        const float* rowC = sp + ((lz + 1) * rowsP + ly + 1) * X;
+        const float4 pc = *reinterpret_cast<const float4*>(rowC + x0);
+        const float pl = x0 > 0 ? rowC[x0 - 1] : pc.x;
+        const float pr = x0 + 4 < X ? rowC[x0 + 4] : pc.w;
+        const float4 pb = *reinterpret_cast<const float4*>((y > 0 ? rowC - X : rowC) + x0);
+        const float4 pt = *reinterpret_cast<const float4*>(rowC + X + x0);
+        const float4 pkv = *reinterpret_cast<const float4*>((z > 0 ? rowC - planeP : rowC) + x0);
+        const float4 pf = *reinterpret_cast<const float4*>((z < Z - 1 ? rowC + planeP : rowC) + x0);
+        const float4 d = *reinterpret_cast<const float4*>(sd + (lz * bx.by + ly) * X + x0);
+        float4 o = fx_jacobi4(c2, pl, pc, pr, pb, pt, pkv, pf, d);
+        if (ROUND) o = make_float4(PStore<__half>::round(o.x), PStore<__half>::round(o.y), PStore<__half>::round(o.z),
+                                   PStore<__half>::round(o.w));
+        return o;
+    };
+    auto gidx = [&](int g) {
+        const int q = g & 0x3ff, ly = (g >> 10) & 0x7ff, lz = g >> 21;
+        return (z0 + lz) * XY + (long long)(y0 + ly) * X + 4 * q;
+    };
+    auto sidx = [&](int g) {
+        const int q = g & 0x3ff, ly = (g >> 10) & 0x7ff, lz = g >> 21;
+        return ((lz + 1) * rowsP + ly + 1) * X + 4 * q;
+    };
+    // halo slot a face group is parked in: the one beyond its face (y rows first: a group on
+    // a y face row belongs to the y list even when it also lies on a z face)
+    auto parked = [&](int g) {
+        const int q = g & 0x3ff;
+        int ly = (g >> 10) & 0x7ff, lz = g >> 21;
+        if (ly == fy0 || ly == fy1) ly = ly == fy0 ? -1 : ny;
+        else lz = lz == fz0 ? -1 : nz;
+        return ((lz + 1) * rowsP + ly + 1) * X + 4 * q;
+    };
+    __syncthreads();
+
+    for (int s = 0; s < n; ++s) {
+        const bool last = s == n - 1;
+        const bool full = s >= n - 2;  // the last two sweeps fill both buffers of the pair
+        void* pout = fx_solve_bufs(S, phase, s).pout;
+        // faces first: computed, then parked in the halo slot next to them (no group reads a
+        // halo slot once the face groups are done) and stored for the neighbours, and the
+        // flag published before the interior is computed. Parking keeps the face values out
+        // of registers while the interior ones are live.
+        {
+            float4 nf[FX_RES_MAXF];
+#pragma unroll
+            for (int k = 0; k < FX_RES_MAXF; ++k)
+                if (pf[k] >= 0) nf[k] = update(fresh(pf[k]));
+            __syncthreads();  // every read of a halo slot is done
+#pragma unroll
+            for (int k = 0; k < FX_RES_MAXF; ++k) {
+                if (pf[k] >= 0) {
+                    *reinterpret_cast<float4*>(sp + parked(fresh(pf[k]))) = nf[k];
+                    if (!last) PStore<PT>::st4(pout, gidx(fresh(pf[k])), nf[k]);
+                }
+            }
+        }
+        if (!last) {
+            __syncthreads();  // every face store of this CTA precedes the flag (release is cumulative)
+            if (t == 0) fx_st_release_u32(cx.flags + b, (unsigned)s + 1);
+        }
+        float4 nv[MAXI];
+#pragma unroll
+        for (int k = 0; k < MAXI; ++k) {
+            if (pi[k] >= 0) nv[k] = update(fresh(pi[k]));
+            asm volatile("" ::: "memory");  // keep each group's loads with its update (register pressure)
+        }
+        __syncthreads();  // every read of the old values is done
+#pragma unroll
+        for (int k = 0; k < MAXI; ++k) {
+            if (pi[k] >= 0) {
+                *reinterpret_cast<float4*>(sp + sidx(fresh(pi[k]))) = nv[k];
+                if (full) PStore<PT>::st4(pout, gidx(fresh(pi[k])), nv[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < FX_RES_MAXF; ++k) {
+            if (pf[k] >= 0) {  // back from the slot this thread parked it in
+                const float4 v = *reinterpret_cast<const float4*>(sp + parked(fresh(pf[k])));
+                *reinterpret_cast<float4*>(sp + sidx(fresh(pf[k]))) = v;
+                if (last) PStore<PT>::st4(pout, gidx(fresh(pf[k])), v);
+            }
+        }
+        if (last) break;
+        if (!fx_res_wait(cx.flags, cx.nb, (unsigned)s, cx.err, &s_flag)) return;
+        fx_res_halo<PT>(cx, pout);
     }
 }

@@ -10,6 +10,7 @@
 // operations as in the WGSL source (shaders.ts, pressureShaders.ts).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 
 #include "fx_internal.h"
@@ -476,7 +477,8 @@ __global__ void __launch_bounds__(256) fxk_norm_partial(const FxSimDev* __restri
 }
 
 // ---- every sweep of a Jacobi phase in one cooperative launch (fx_jacobi_res.cuh) --------
-template <typename PT>
+// VARIANT: 0 column, 1 faces-first, 2 faces-first for small boxes (fx_jacobi_res.cuh).
+template <typename PT, int VARIANT>
 __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatchDev* __restrict__ B, int phase) {
     extern __shared__ float4 fx_res_smem[];
     const int w = blockIdx.x;
@@ -484,8 +486,11 @@ __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatc
     const int si = fx_find_sim(B->start[FX_SHAPE_RES], B->nsims, w);
     const FxSimDev& S = *B->sims[si];
     if (!S.active) return;
-    fx_res_box<PT, sizeof(PT) == 2>(S, B->res[si], w - B->start[FX_SHAPE_RES][si], phase,
-                                    reinterpret_cast<float*>(fx_res_smem));
+    float* sm = reinterpret_cast<float*>(fx_res_smem);
+    const int b = w - B->start[FX_SHAPE_RES][si];
+    if (VARIANT == 1) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI>(S, B->res[si], b, phase, sm);
+    else if (VARIANT == 2) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI_SMALL>(S, B->res[si], b, phase, sm);
+    else fx_res_box_col<PT, sizeof(PT) == 2>(S, B->res[si], b, phase, sm);
 }
 
 __global__ void fxk_norm_final(const double* __restrict__ partial, int nblocks, double* __restrict__ out) {
@@ -631,23 +636,37 @@ bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, 
     return false;
 }
 
-// Largest resident-Jacobi grid that one cooperative launch can keep resident.
-int fx_res_capacity(bool half) {
-    const void* fn = half ? (const void*)fxk_jacobi_res<__half> : (const void*)fxk_jacobi_res<float>;
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FX_RES_THREADS, FX_RES_SMEM_MAX) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return per_sm * num_sms();
+template <typename PT, int VARIANT>
+static const void* res_fn() {
+    return (const void*)fxk_jacobi_res<PT, VARIANT>;
+}
+static const void* res_kernel(bool half, int variant) {
+    if (half) return variant == 1 ? res_fn<__half, 1>() : (variant == 2 ? res_fn<__half, 2>() : res_fn<__half, 0>());
+    return variant == 1 ? res_fn<float, 1>() : (variant == 2 ? res_fn<float, 2>() : res_fn<float, 0>());
 }
 
-cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, const FxBatchDev* B, int ctas, int phase, int smem) {
-    const void* fn = half ? (const void*)fxk_jacobi_res<__half> : (const void*)fxk_jacobi_res<float>;
+// Largest resident-Jacobi grid that one cooperative launch can keep resident.
+int fx_res_capacity(bool half) {
+    int cap = 1 << 30;
+    for (int variant = 0; variant < 3; ++variant) {  // every variant: the plan picks one later
+        const void* fn = res_kernel(half, variant);
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FX_RES_THREADS, FX_RES_SMEM_MAX) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
+        cap = std::min(cap, per_sm * num_sms());
+    }
+    return cap;
+}
+
+cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, int variant, const FxBatchDev* B, int ctas, int phase,
+                                 int smem) {
+    const void* fn = res_kernel(half, variant);
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
@@ -660,8 +679,8 @@ cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, const FxBatchDev* B,
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (half) return cudaLaunchKernelEx(&cfg, fxk_jacobi_res<__half>, B, phase);
-    return cudaLaunchKernelEx(&cfg, fxk_jacobi_res<float>, B, phase);
+    void* args[] = {(void*)&B, (void*)&phase};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase) {
