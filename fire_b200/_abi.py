@@ -43,7 +43,10 @@ FIELD_LIQUID = 5
 FIELD_EMITTER_MASK = 6
 FIELD_CORRECTION = 7
 FIELD_FINAL_DIVERGENCE = 8
-FIELD_COUNT = 9
+FIELD_RENDER_FLOW = 9
+FIELD_RENDER_CHEMISTRY = 10
+FIELD_RENDER_MEDIA = 11
+FIELD_COUNT = 12
 
 JACOBI_AUTO = 0
 JACOBI_UNBLOCKED = 1
@@ -67,6 +70,9 @@ FIELD_LAYOUT = {
     FIELD_EMITTER_MASK: ("uint8", 1),
     FIELD_CORRECTION: ("float32", 1),
     FIELD_FINAL_DIVERGENCE: ("float32", 1),
+    FIELD_RENDER_FLOW: ("uint16", 4),
+    FIELD_RENDER_CHEMISTRY: ("uint16", 4),
+    FIELD_RENDER_MEDIA: ("uint16", 4),
 }
 
 FIELD_NAMES = {
@@ -79,6 +85,9 @@ FIELD_NAMES = {
     "emitter_mask": FIELD_EMITTER_MASK,
     "correction": FIELD_CORRECTION,
     "final_divergence": FIELD_FINAL_DIVERGENCE,
+    "render_flow": FIELD_RENDER_FLOW,
+    "render_chemistry": FIELD_RENDER_CHEMISTRY,
+    "render_media": FIELD_RENDER_MEDIA,
 }
 
 
@@ -153,6 +162,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_write_field": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_divergence_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
         "firex_read_field_async": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
+        "firex_set_render_packing": (C.c_int, [vp, C.c_int32]),
+        "firex_render_volumes": (C.c_int, [vp, C.POINTER(C.c_void_p)]),
         "firex_divergence_norm_noalloc": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float), vp,
                                                     C.POINTER(C.c_double)]),
         "firex_get_state": (C.c_int, [vp, C.POINTER(State)]),
@@ -190,6 +201,7 @@ HEADER_SYMBOLS = [
     "firex_default_options", "firex_field_element_size", "firex_create", "firex_destroy",
     "firex_last_error", "firex_set_parameter", "firex_get_parameter", "firex_reset", "firex_step",
     "firex_sync", "firex_read_field", "firex_read_field_async", "firex_write_field", "firex_divergence_norm",
+    "firex_set_render_packing", "firex_render_volumes",
     "firex_divergence_norm_noalloc", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_stream", "firex_set_profiling", "firex_pass_times",

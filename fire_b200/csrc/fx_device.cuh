@@ -54,7 +54,7 @@ enum FxSlot {
     U_DT = 4, U_TIME = 5,
     U_FUEL_RATE = 8, U_OXYGEN = 9, U_HEAT_EFF = 10, U_VORTICITY = 11,
     U_T_AMBIENT = 15,
-    U_AIM_HEIGHT = 25,
+    U_VIEW_MODE = 24, U_AIM_HEIGHT = 25,
     U_BURNER_X = 28, U_BURNER_Z = 29, U_THICKNESS = 30, U_FIRE_POWER = 31,
     U_DOMAIN_X = 32, U_DOMAIN_Y = 33, U_DOMAIN_Z = 34,
     U_LIFT = 36, U_BUOYANCY = 37, U_PERSISTENCE = 38,
@@ -163,6 +163,9 @@ struct __align__(16) FxSimDev {
     uint32_t* liquid;
     float* tab;            // per-step tables of simulate (fx_step_math.cuh)
     FxDivc divc[DIVC_COUNT];
+    uint2* render[3];      // render volumes (4 x FP16 per cell): flow, chemistry, media
+    int renderPack;        // 1: the step ends by packing the render volumes
+    int renderPad;
     unsigned* sync;        // [2]: error word (a bounded device wait expired); from
                            // FX_RES_FLAGS: the resident Jacobi's per-box flags of both
                            // phases (zeroed at every step start)

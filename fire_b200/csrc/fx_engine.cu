@@ -129,12 +129,14 @@ struct StepPlan {
     int zmZc = 16;            // z planes per CTA of the single-sweep (z-marching) kernel
     bool row4 = false;        // single sweeps by the unblocked kernel instead
     bool fuseP = false, fuseR = false;
+    bool pack = false;        // a member packs its render volumes at the end of every step
     bool res = false;         // every sweep of a phase in one resident launch
     int resVariant = 0;       // ... by this variant of the kernel
     int resSmem = 0;          // its dynamic shared memory per CTA
     int bricks[FX_NSHAPES] = {};
     auto key() const {
-        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, res, resVariant, resSmem, bricks[0],
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, res, resVariant, resSmem,
+                        bricks[0],
                         bricks[1], bricks[2], bricks[3], bricks[4], bricks[5]);
     }
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
@@ -181,6 +183,7 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     enqueue_jacobi_phase(st, pl, B, 1);
     fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 1);
     fx_launch_step_end(st, B);
+    if (pl.pack) fx_launch_pack_batch(st, B, pl.bricks[FX_SHAPE_ROW4]);
 }
 
 // Jacobi kernel when the caller did not choose one (measured on B200, 96+96 sweeps):
@@ -377,6 +380,17 @@ struct firex_sim {
         poisoned = true;
         err = std::string(what) + ": " + cudaGetErrorString(e);
         return FIREX_ERR_CUDA;
+    }
+
+    // The three render volumes (8 B per cell each), allocated on first use.
+    bool ensure_render_volumes() {
+        if (h.render[0]) return true;
+        for (int k = 0; k < 3; ++k) {
+            h.render[k] = (uint2*)alloc((size_t)N * 8);
+            if (!h.render[k]) return false;
+        }
+        dirty = true;
+        return true;
     }
 
     // After a stream synchronisation: whether a bounded device wait of this simulation
@@ -607,6 +621,7 @@ struct firex_batch {
             uniformP = uniformP && s->h.P == members[0]->h.P;
             uniformR = uniformR && s->h.R == members[0]->h.R;
             cells += s->N;
+            p.pack = p.pack || s->h.renderPack != 0;
         }
         const bool own = jacobiKernel != FIREX_JACOBI_AUTO;
         int kernel = own ? jacobiKernel : members[0]->jacobiKernel;
@@ -703,7 +718,8 @@ struct firex_batch {
         fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 1);
         mark(FIREX_PASS_PROJECT, 1);
         fx_launch_step_end(stream, d);
-        mark(FIREX_PASS_OTHER, 1);
+        if (pl.pack) fx_launch_pack_batch(stream, d, pl.bricks[FX_SHAPE_ROW4]);
+        mark(FIREX_PASS_OTHER, pl.pack ? 2 : 1);
     }
 
     cudaError_t graph_for(const StepPlan& pl, cudaGraphExec_t* out) {
@@ -764,7 +780,7 @@ struct firex_batch {
             if (e != cudaSuccess) return poison(e, "step");
             for (firex_sim* s : members) s->advance_mirror();
             if (!profiling) {
-                pendingLaunches[FIREX_PASS_OTHER] += 3;
+                pendingLaunches[FIREX_PASS_OTHER] += pl.pack ? 4 : 3;
                 pendingLaunches[FIREX_PASS_SIMULATE] += 1;
                 pendingLaunches[FIREX_PASS_DIVERGENCE] += 2;
                 pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
@@ -915,6 +931,9 @@ size_t firex_field_element_size(int32_t field) {
         case FIREX_FIELD_CORRECTION:
         case FIREX_FIELD_FINAL_DIVERGENCE: return 4;
         case FIREX_FIELD_EMITTER_MASK: return 1;
+        case FIREX_FIELD_RENDER_FLOW:
+        case FIREX_FIELD_RENDER_CHEMISTRY:
+        case FIREX_FIELD_RENDER_MEDIA: return 8;
     }
     return 0;
 }
@@ -1136,7 +1155,12 @@ int firex_read_field(firex_sim* s, int32_t field, void* host, size_t bytes) {
     cudaStream_t st = s->stream();
     cudaError_t e = cudaSuccess;
     const size_t N = (size_t)s->N;
-    if (field == FIREX_FIELD_EMITTER_MASK || field == FIREX_FIELD_FINAL_DIVERGENCE) {
+    if (field >= FIREX_FIELD_RENDER_FLOW && field <= FIREX_FIELD_RENDER_MEDIA) {
+        if (!s->ensure_render_volumes()) return s->fail(FIREX_ERR_OOM, "render volumes: device allocation failed");
+        s->flush(st);
+        fx_launch_pack_sim(st, s->d);
+        e = cudaMemcpyAsync(host, s->h.render[field - FIREX_FIELD_RENDER_FLOW], bytes, cudaMemcpyDeviceToHost, st);
+    } else if (field == FIREX_FIELD_EMITTER_MASK || field == FIREX_FIELD_FINAL_DIVERGENCE) {
         s->flush(st);
         if (field == FIREX_FIELD_EMITTER_MASK) fx_launch_emitter_mask(st, s->d, (uint8_t*)s->d_tmp);
         else fx_launch_final_divergence(st, s->d, (float*)s->d_tmp);
@@ -1206,7 +1230,8 @@ int firex_write_field(firex_sim* s, int32_t field, const void* host, size_t byte
     const size_t es = firex_field_element_size(field);
     if (!es) return s->fail(FIREX_ERR_BAD_ARG, "unknown field id");
     if (bytes != es * (size_t)s->N) return s->fail(FIREX_ERR_BAD_ARG, "byte count does not match the field size");
-    if (field == FIREX_FIELD_EMITTER_MASK || field == FIREX_FIELD_FINAL_DIVERGENCE || field == FIREX_FIELD_CORRECTION)
+    if (field == FIREX_FIELD_EMITTER_MASK || field == FIREX_FIELD_FINAL_DIVERGENCE || field == FIREX_FIELD_CORRECTION ||
+        field >= FIREX_FIELD_RENDER_FLOW)
         return s->fail(FIREX_ERR_BAD_ARG, "field is read only");
     DeviceGuard dg(s->device);
     cudaStream_t st = s->stream();
@@ -1336,7 +1361,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_block = p.k;
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
-    out->launches_per_step = 8 + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+    out->launches_per_step = 8 + (p.pack ? 1 : 0) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     return FIREX_OK;
@@ -1360,6 +1385,22 @@ int firex_batch_set_jacobi(firex_batch* b, int32_t kernel, int32_t block, int32_
     b->jacobiKernel = kernel;
     b->jacobiK = kernel == FIREX_JACOBI_FUSED ? block : 1;
     b->jacobiZc = zchunk;
+    return FIREX_OK;
+}
+
+int firex_set_render_packing(firex_sim* s, int32_t on) {
+    if (!s) return FIREX_ERR_BAD_ARG;
+    if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
+    DeviceGuard dg(s->device);
+    if (on && !s->ensure_render_volumes()) return s->fail(FIREX_ERR_OOM, "render volumes: device allocation failed");
+    s->h.renderPack = on ? 1 : 0;
+    s->dirty = true;
+    return FIREX_OK;
+}
+
+int firex_render_volumes(const firex_sim* s, void* out[3]) {
+    if (!s || !out) return FIREX_ERR_BAD_ARG;
+    for (int k = 0; k < 3; ++k) out[k] = s->h.render[k];
     return FIREX_OK;
 }
 

@@ -37,6 +37,9 @@ int fx_res_capacity(bool half);
 void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbient, float oxygen, float noise);
 void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask);
 void fx_launch_final_divergence(cudaStream_t s, const FxSimDev* S, float* out);
+// Render volumes: one simulation (a read), or every packing member of a batch (step end).
+void fx_launch_pack_sim(cudaStream_t s, const FxSimDev* S);
+void fx_launch_pack_batch(cudaStream_t s, const FxBatchDev* B, int bricks);
 int fx_norm_partial_blocks(long long cells);
 void fx_launch_divergence_norm(cudaStream_t s, const FxSimDev* S, long long cells, double* partial, double* out);
 void fx_launch_upload_desc(cudaStream_t s, const FxSimDev& host, FxSimDev* dev);

@@ -419,6 +419,76 @@ __global__ void fxk_emitter_mask(const FxSimDev* __restrict__ S, uint8_t* __rest
     }
 }
 
+// ---- render-field packing (storePackedFields, qualityShaders.ts:37-75) --------------------
+// The three rgba16float volumes of the canonical state as FP16 (round to nearest even):
+// flow (u, v, w, clamp((T - 300) / 2600, 0, 1)), chemistry (max(species, 0)) and media
+// (reaction, soot, liquid, display value). In view 7 the display value is the divergence of
+// the canonical flow the presentation computes (FireXEngine.ts:2588-2596), 0 on the outer
+// shell. Headless device buffers stand in for the reference's textures.
+FXD uint2 fx_half4(float a, float b, float c, float d) {
+    const __half2 lo = __floats2half2_rn(a, b), hi = __floats2half2_rn(c, d);
+    uint2 r;
+    r.x = *reinterpret_cast<const uint32_t*>(&lo);
+    r.y = *reinterpret_cast<const uint32_t*>(&hi);
+    return r;
+}
+FXD void fx_pack_cell(const FxSimDev& S, int id, int x, int y, int z, bool view7, const float3& m) {
+    const float4* flow = reinterpret_cast<const float4*>(S.flow[S.fi]);
+    const float4 f = __ldg(flow + id);
+    const float4 sr = S.storage == FX_STORAGE_MIXED ? StMixed::ld_species(S.species[S.si], id)
+                                                    : StF32::ld_species(S.species[S.si], id);
+    const float4 sp = make_float4(fx_max(sr.x, 0.0f), fx_max(sr.y, 0.0f), fx_max(sr.z, 0.0f), fx_max(sr.w, 0.0f));
+    const float reaction = fx_clamp(__ldg(S.reaction + id), 0.0f, 4.0f);
+    const float richness = fx_clamp(sp.x / fx_max(sp.x + sp.y * 0.25f, FC(0.0001)), 0.0f, 1.0f);
+    const float soot = sp.z * fx_smoothstep(0.25f, FC(0.82), richness);
+    const float liq = (float)__ldg(S.liquid + id) * FC(3.4 / 4096.0);
+    float disp = fx_max(fx_max(reaction, soot), fx_max(liq, fx_max(sp.w, fx_smoothstep(420.0f, 700.0f, f.w))));
+    if (view7) {
+        const bool shell = x == 0 || y == 0 || z == 0 || x + 1 >= S.X || y + 1 >= S.Y || z + 1 >= S.Z;
+        if (shell) {
+            disp = 0.0f;
+        } else {
+            const float l = __ldg(flow + id - 1).x;
+            const float bo = __ldg(flow + id - S.X).y;
+            const float ba = __ldg(flow + id - S.X * S.Y).z;
+            disp = (f.x - l) * m.x + (f.y - bo) * m.y + (f.z - ba) * m.z;
+        }
+    }
+    S.render[0][id] = fx_half4(f.x, f.y, f.z, fx_clamp((f.w - 300.0f) / 2600.0f, 0.0f, 1.0f));
+    S.render[1][id] = fx_half4(sp.x, sp.y, sp.z, sp.w);
+    S.render[2][id] = fx_half4(reaction, soot, liq, disp);
+}
+FXD bool fx_view7(const float* u) { return (unsigned)fx_clamp(rintf(u[U_VIEW_MODE]), 0.0f, 7.0f) == 7u; }
+
+// One simulation's volumes (a read of a render field).
+__global__ void fxk_pack_sim(const FxSimDev* __restrict__ Sp) {
+    const FxSimDev& S = *Sp;
+    const int n = S.X * S.Y * S.Z;
+    const float3 m = fx_metric(S.prm.u);
+    const bool v7 = fx_view7(S.prm.u);
+    for (int id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+        const int x = id % S.X, t = id / S.X, y = t % S.Y, z = t / S.Y;
+        fx_pack_cell(S, id, x, y, z, v7, m);
+    }
+}
+
+// Every member that packs each step, after the step's end (canonical buffers current).
+__global__ void __launch_bounds__(256) fxk_pack_batch(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+        if (!S.renderPack) return;
+        const Lane4 r = fx_lane4(S, b);
+        if (r.n <= 0) return;
+        const int lane = threadIdx.x & 31;
+        const float3 m = fx_metric(S.prm.u);
+        const bool v7 = fx_view7(S.prm.u);
+        int xs[4], ys[4], zs[4];
+        fx_lane4_coords(S, r, xs, ys, zs);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            if (lane + 32 * i < r.n) fx_pack_cell(S, r.c0 + 32 * i, xs[i], ys[i], zs[i], v7, m);
+    });
+}
+
 // Divergence of the canonical flow F[fi] into out (the FINAL_DIVERGENCE field).
 __global__ void fxk_final_divergence(const FxSimDev* __restrict__ S, float* __restrict__ out) {
     const long long n = (long long)S->X * S->Y * S->Z;
@@ -700,6 +770,12 @@ void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbie
 
 void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask) {
     fxk_emitter_mask<<<num_sms() * 8, 256, 0, s>>>(S, mask);
+}
+
+void fx_launch_pack_sim(cudaStream_t s, const FxSimDev* S) { fxk_pack_sim<<<num_sms() * 8, 256, 0, s>>>(S); }
+void fx_launch_pack_batch(cudaStream_t s, const FxBatchDev* B, int bricks) {
+    static int g = persistent_grid((const void*)fxk_pack_batch, 256, 1 << 30);
+    fxk_pack_batch<<<row4_grid(g, bricks), 256, 0, s>>>(B);
 }
 
 void fx_launch_final_divergence(cudaStream_t s, const FxSimDev* S, float* out) {

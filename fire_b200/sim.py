@@ -228,6 +228,16 @@ class FireXSim(_Handle):
     def __init__(self, dims: Iterable[int], options: A.Options | None = None, **kw):
         super().__init__(load_library(), dims, options, **kw)
 
+    def set_render_packing(self, on: bool) -> None:
+        """Pack the three FP16 render volumes at the end of every step (qualityShaders.ts)."""
+        self._check(self._lib.firex_set_render_packing(self._h, 1 if on else 0))
+
+    def render_volumes(self) -> list:
+        """Device addresses of the render volumes (flow, chemistry, media); 0 before use."""
+        out = (C.c_void_p * 3)()
+        self._check(self._lib.firex_render_volumes(self._h, out))
+        return [v or 0 for v in out]
+
     def read_async(self, field, out: np.ndarray) -> np.ndarray:
         """Starts an overlapped copy of `field` (as it stands after the steps enqueued so
         far) into `out`; `out` is complete after sync(). Use pinned memory for overlap."""

@@ -107,7 +107,12 @@ void firex_default_options(firex_options* opt);
 #define FIREX_FIELD_EMITTER_MASK 6     /* uint8 per cell, read only: sphere emitter mask */
 #define FIREX_FIELD_CORRECTION 7       /* float per cell: last residual-pressure result */
 #define FIREX_FIELD_FINAL_DIVERGENCE 8 /* float per cell, read only: divergence of FLOW */
-#define FIREX_FIELD_COUNT 9
+/* The three render volumes (storePackedFields, qualityShaders.ts:37-75), read only: 4 FP16
+ * values per cell (round to nearest even), as the reference's rgba16float textures hold. */
+#define FIREX_FIELD_RENDER_FLOW 9      /* u, v, w, clamp((T - 300) / 2600, 0, 1) */
+#define FIREX_FIELD_RENDER_CHEMISTRY 10 /* max(species, 0) */
+#define FIREX_FIELD_RENDER_MEDIA 11    /* reaction, soot, liquid, display value (view 7: divergence) */
+#define FIREX_FIELD_COUNT 12
 
 /* Element size in bytes of a field (16, 4 or 1), or 0 for an unknown id. */
 size_t firex_field_element_size(int32_t field);
@@ -176,6 +181,15 @@ int firex_write_field(firex_sim* sim, int32_t field, const void* host, size_t by
  * refused with FIREX_ERR_UNSUPPORTED: use firex_read_field. The first call allocates the
  * staging buffer (16 B/cell) and the copy stream. */
 int firex_read_field_async(firex_sim* sim, int32_t field, void* host, size_t bytes);
+
+/* Render volumes. Replaces packFields / copyAndPackBeautyFields (qualityShaders.ts:65-87),
+ * whose rgba16float textures become three device buffers of 4 x FP16 per cell (cell index
+ * x + X*(y + Y*z)) in the order of FIREX_FIELD_RENDER_FLOW, _CHEMISTRY, _MEDIA. With
+ * packing on, every step ends by packing them from the canonical state; reading a render
+ * field packs them on demand either way. firex_render_volumes gives their device
+ * addresses (NULL until first allocated) for a renderer on the same device. */
+int firex_set_render_packing(firex_sim* sim, int32_t on);
+int firex_render_volumes(const firex_sim* sim, void* out[3]);
 
 /* Post-projection divergence of FLOW over interior cells (the one-cell outer shell is
  * excluded, qualityShaders.ts:47-57), reduced in FP64: out[0] = L2 norm, out[1] = max

@@ -850,8 +850,57 @@ struct Sim : SimBase {
                 divergence_pass(g, flow[0].data(), d.data());
                 return copy_out_scalar(d, out, bytes);
             }
+            case FIREX_FIELD_RENDER_FLOW:
+            case FIREX_FIELD_RENDER_CHEMISTRY:
+            case FIREX_FIELD_RENDER_MEDIA:
+                if (bytes != N * 8) return FIREX_ERR_BAD_ARG;
+                render_pack(field - FIREX_FIELD_RENDER_FLOW, (uint16_t*)out);
+                return FIREX_OK;
         }
         return FIREX_ERR_BAD_ARG;
+    }
+
+    // storePackedFields / packFields (qualityShaders.ts:37-75): the three rgba16float render
+    // volumes of the canonical state, as FP16 bits (round to nearest even). which: 0 flow
+    // (u, v, w, normalised T), 1 chemistry (species), 2 media (reaction, soot, liquid,
+    // display value). In view 7 the display value is the post-projection divergence the
+    // presentation computes from flow[0] (FireXEngine.ts:2588-2596), 0 on the outer shell.
+    void render_pack(int which, uint16_t* out) {
+        float u[44];
+        write_uniforms(u, named, X, Y, Z, 0.0, simulationTime, frameIndex, opt.cinematic);
+        const bool view7 = (unsigned)clampT(std::nearbyint(u[24]), 0.0f, 7.0f) == 7u;
+        std::vector<T> d;
+        if (view7) {
+            d.resize(N);
+            Grid<T> g = grid(0.0);
+            divergence_pass(g, flow[0].data(), d.data());
+        }
+        const V4<T>* sp = species[speciesIndex].data();
+        for (int z = 0; z < Z; ++z)
+            for (int y = 0; y < Y; ++y)
+                for (int x = 0; x < X; ++x) {
+                    const size_t id = (size_t)x + (size_t)X * ((size_t)y + (size_t)Y * z);
+                    const V4<T> f = flow[0][id];
+                    const V4<T> sr = sp[id];
+                    const V4<T> spc = {std::max(sr.x, T(0)), std::max(sr.y, T(0)), std::max(sr.z, T(0)), std::max(sr.w, T(0))};
+                    const T reaction = clampT(this->reaction[id], T(0), T(4));
+                    const T richness = clampT(spc.x / std::max(spc.x + spc.y * T(0.25), T(0.0001)), T(0), T(1));
+                    const T soot = spc.z * smoothstepT(T(0.25), T(0.82), richness);
+                    const T liq = T(float(liquid[id])) * T(3.4 / 4096.0);
+                    const bool shell = x == 0 || y == 0 || z == 0 || x + 1 >= X || y + 1 >= Y || z + 1 >= Z;
+                    T disp = std::max(std::max(reaction, soot),
+                                      std::max(liq, std::max(spc.w, smoothstepT(T(420.0), T(700.0), f.w))));
+                    if (view7) disp = shell ? T(0) : d[id];
+                    T v[4];
+                    if (which == 0) {
+                        v[0] = f.x, v[1] = f.y, v[2] = f.z, v[3] = clampT((f.w - T(300.0)) / T(2600.0), T(0), T(1));
+                    } else if (which == 1) {
+                        v[0] = spc.x, v[1] = spc.y, v[2] = spc.z, v[3] = spc.w;
+                    } else {
+                        v[0] = reaction, v[1] = soot, v[2] = liq, v[3] = disp;
+                    }
+                    for (int k = 0; k < 4; ++k) out[4 * id + k] = f32_to_f16((float)v[k]);
+                }
     }
 
     int write_vec4(std::vector<V4<T>>& v, const void* in, size_t bytes) {

@@ -169,7 +169,7 @@ def test_library_host_only_entry_points():
     lib.firex_default_options(C.byref(o))
     assert (o.precision, o.pressure_mode, o.pressure_iterations, o.correction_iterations, o.cinematic) == (
         A.PRECISION_F32, A.PRESSURE_AUTO, 64, 64, 1)
-    assert [lib.firex_field_element_size(f) for f in range(A.FIELD_COUNT)] == [16, 16, 4, 4, 4, 4, 1, 4, 4]
+    assert [lib.firex_field_element_size(f) for f in range(A.FIELD_COUNT)] == [16, 16, 4, 4, 4, 4, 1, 4, 4, 8, 8, 8]
     assert lib.firex_field_element_size(99) == 0
     for dims in ((508, 508, 508), (1020, 256, 256), (1024, 256, 256), (64, 96, 64)):
         assert lib.firex_reference_memory_estimate(A.DIMS(*dims), 4096) == G.estimateFireXGridMemory(dims, 4096).totalBytes
