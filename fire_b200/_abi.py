@@ -116,7 +116,8 @@ class Options(C.Structure):
         ("jacobi_block", C.c_int32),
         ("memory_budget_bytes", C.c_uint64),
         ("jacobi_zchunk", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("particle_count", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -164,6 +165,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_read_field_async": (C.c_int, [vp, C.c_int32, vp, C.c_size_t]),
         "firex_set_render_packing": (C.c_int, [vp, C.c_int32]),
         "firex_render_volumes": (C.c_int, [vp, C.POINTER(C.c_void_p)]),
+        "firex_read_particles": (C.c_int, [vp, vp, C.c_size_t]),
+        "firex_write_particles": (C.c_int, [vp, vp, C.c_size_t]),
         "firex_divergence_norm_noalloc": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float), vp,
                                                     C.POINTER(C.c_double)]),
         "firex_get_state": (C.c_int, [vp, C.POINTER(State)]),
@@ -201,7 +204,7 @@ HEADER_SYMBOLS = [
     "firex_default_options", "firex_field_element_size", "firex_create", "firex_destroy",
     "firex_last_error", "firex_set_parameter", "firex_get_parameter", "firex_reset", "firex_step",
     "firex_sync", "firex_read_field", "firex_read_field_async", "firex_write_field", "firex_divergence_norm",
-    "firex_set_render_packing", "firex_render_volumes",
+    "firex_set_render_packing", "firex_render_volumes", "firex_read_particles", "firex_write_particles",
     "firex_divergence_norm_noalloc", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_stream", "firex_set_profiling", "firex_pass_times",
@@ -210,4 +213,4 @@ HEADER_SYMBOLS = [
     "firex_batch_last_error", "firex_batch_stream",
 ]
 
-PASS_NAMES = ("simulate", "divergence", "jacobi", "project", "other")
+PASS_NAMES = ("simulate", "divergence", "jacobi", "project", "other", "particles")

@@ -163,6 +163,12 @@ struct __align__(16) FxSimDev {
     uint32_t* liquid;
     float* tab;            // per-step tables of simulate (fx_step_math.cuh)
     FxDivc divc[DIVC_COUNT];
+    float4* part[2];       // droplets (2 float4 each: position + age, velocity + mass), ping-pong
+    float4* pdens;         // droplet density, near density, pressure, near pressure
+    int np;                // droplet count
+    int pti;               // droplets of the current state: part[pti]
+    int water;             // 1: the particle passes run in this step (waterEnabled, waterFlow > 0.001)
+    int waterPad;
     uint2* render[3];      // render volumes (4 x FP16 per cell): flow, chemistry, media
     int renderPack;        // 1: the step ends by packing the render volumes
     int renderPad;
@@ -182,7 +188,8 @@ enum FxShape {
     FX_SHAPE_ZM = 3,
     FX_SHAPE_TAB = 4,
     FX_SHAPE_RES = 5,  // one CTA per box of the resident Jacobi (fx_jacobi_res.cuh)
-    FX_NSHAPES = 6
+    FX_SHAPE_PART = 6, // FX_SPH_THREADS droplets per brick (members whose water runs)
+    FX_NSHAPES = 7
 };
 
 // Box decomposition of one simulation for the resident Jacobi: boxes of by x bz rows of
@@ -199,6 +206,7 @@ struct FxResBox {
 #define FX_CELL_BY 4
 #define FX_CELL_BZ 2
 #define FX_ROW4_THREADS 256
+#define FX_SPH_THREADS 128  // droplets per brick of the particle passes
 
 struct FxBatchDev {
     int nsims;

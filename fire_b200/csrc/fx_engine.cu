@@ -137,7 +137,7 @@ struct StepPlan {
     auto key() const {
         return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, res, resVariant, resSmem,
                         bricks[0],
-                        bricks[1], bricks[2], bricks[3], bricks[4], bricks[5]);
+                        bricks[1], bricks[2], bricks[3], bricks[4], bricks[5], bricks[6]);
     }
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
 };
@@ -172,9 +172,13 @@ void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, in
     }
 }
 
+// Launches of the droplet pass (clear, density, integrate, deposit) when a member sprays.
+int sph_launches(const StepPlan& pl) { return pl.bricks[FX_SHAPE_PART] > 0 ? 4 : 0; }
+
 void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     fx_launch_step_begin(st, B);
     fx_launch_step_tables(st, B, pl.bricks[FX_SHAPE_TAB]);
+    if (sph_launches(pl)) fx_launch_sph(st, B, pl.bricks[FX_SHAPE_ROW4], pl.bricks[FX_SHAPE_PART]);
     fx_launch_simulate(st, pl.storage, B, pl.bricks[FX_SHAPE_CELL]);
     fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 0);
     enqueue_jacobi_phase(st, pl, B, 0);
@@ -418,13 +422,14 @@ struct firex_sim {
         return p;
     }
 
-    static size_t planned_bytes(int X, int Y, int Z, int storage, int mode) {
+    static size_t planned_bytes(int X, int Y, int Z, int storage, int mode, int particles) {
         const long long N = (long long)X * Y * Z;
         const size_t species = storage == FX_STORAGE_MIXED ? 8 : 16;
         const size_t pbytes = mode == FIREX_PRESSURE_F16 ? 2 : 4;
         const size_t npress = mode == FIREX_PRESSURE_COLD_F32 ? 2 : 4;
         const size_t per = 16 * 2 + species * 2 + pbytes * npress + 4 /*div*/ + 4 /*reaction*/ + 4 /*liquid*/ + 4 /*tmp*/;
-        return (size_t)N * per + (size_t)fx_tab_layout(X, Y, Z).total * 4 + sizeof(FxSimDev) + 64 * 1024;
+        return (size_t)N * per + (size_t)fx_tab_layout(X, Y, Z).total * 4 + sizeof(FxSimDev) + 64 * 1024 +
+               (size_t)std::max(0, particles) * (2 * 32 + 16);  // two droplet buffers and their densities
     }
     size_t table_bytes() const { return (size_t)fx_tab_layout(X, Y, Z).total * 4;
     }
@@ -444,7 +449,7 @@ struct firex_sim {
             P("fuelRate"), P("oxygenRate"), P("heatEfficiency"), P("vorticity"),
             P("waterFlow"), (P("sprayAngle") * M_PI) / 180, P("waterEnabled") != 0 ? 1.0 : 0.0, 300,
             P("cameraYaw"), P("cameraPitch"), P("cameraDistance"), 1,  // canvas aspect (presentation only)
-            1, 1, 0, 0,                                                // canvas size, rays, particles
+            1, 1, 0, (double)std::max(0, opt.particle_count),          // canvas size, rays, particles
             P("viewMode"), P("aimHeight"), P("nozzleType"), P("exposure"),
             P("burnerSize"), P("burnerDepth"), P("sourceThickness"), P("firePower"),
             P("domainWidth"), P("domainHeight"), P("domainDepth"), 0,
@@ -509,6 +514,31 @@ struct firex_sim {
         h.fi ^= 1;
         h.si ^= 1;
         h.pi = (h.mode == FIREX_PRESSURE_COLD_F32) ? (h.P & 1) : (h.pi ^ (h.P & 1));
+        if (h.water) h.pti ^= 1;
+    }
+
+    // ---- droplets (SPH): host-side state of FireXEngine.ts:2158-2171 ----
+    bool particleFieldActive = false, liquidMayContainWater = false;
+    std::vector<float> hostParticles;  // staging of the initial state (kept alive for the async copy)
+    bool water_active() const { return named[param_slot("waterEnabled")] != 0 && named[param_slot("waterFlow")] > 0.001; }
+    // writeParticleInitialState (FireXEngine.ts:1976-2034), into both droplet buffers
+    void write_particle_initial_state(cudaStream_t st, bool active);
+    // Before each step: the transitions of the reference's particle state machine.
+    void prepare_particles(cudaStream_t st) {
+        if (h.np <= 0) return;
+        const bool on = water_active();
+        if (on) {
+            if (!particleFieldActive) write_particle_initial_state(st, true);
+            liquidMayContainWater = true;
+        } else if (liquidMayContainWater || particleFieldActive) {
+            cudaMemsetAsync(h.liquid, 0, (size_t)N * 4, st);
+            write_particle_initial_state(st, false);
+            liquidMayContainWater = false;
+        }
+        if ((h.water != 0) != on) {
+            h.water = on ? 1 : 0;
+            dirty = true;
+        }
     }
 
     int reset();
@@ -532,6 +562,7 @@ struct firex_batch {
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;  // batch override (AUTO: first member's)
     int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
     int tableRes = -1;                               // whether resident boxes were requested
+    std::vector<char> tableWater;                    // which members sprayed when the table was filled
     bool resOk = false;                              // ... and the batch fits one resident launch
     int resVariant = 0;                              // ... of this kernel variant
     int resSmem = 0;
@@ -586,6 +617,8 @@ struct firex_batch {
             h->start[FX_SHAPE_ZM][i] = acc[FX_SHAPE_ZM];
             h->start[FX_SHAPE_TAB][i] = acc[FX_SHAPE_TAB];
             h->start[FX_SHAPE_RES][i] = acc[FX_SHAPE_RES];
+            h->start[FX_SHAPE_PART][i] = acc[FX_SHAPE_PART];
+            acc[FX_SHAPE_PART] += s->h.water ? (s->h.np + FX_SPH_THREADS - 1) / FX_SPH_THREADS : 0;
             if (resOk) {
                 h->res[i] = boxes[i];
                 acc[FX_SHAPE_RES] += boxes[i].nby * boxes[i].nbz;
@@ -604,7 +637,14 @@ struct firex_batch {
         tableZc = zc;
         tableZmZc = zmZc;
         tableRes = wantRes ? 1 : 0;
+        tableWater = water_signature();
         tableDirty = true;
+    }
+
+    std::vector<char> water_signature() const {
+        std::vector<char> w;
+        for (firex_sim* s : members) w.push_back(s->h.water ? 1 : 0);
+        return w;
     }
 
     StepPlan plan() {
@@ -645,7 +685,8 @@ struct firex_batch {
         if (!p.fuseP && !p.fuseR) p.k = 1;
         p.row4 = kernel == FIREX_JACOBI_UNBLOCKED;
         p.zmZc = (kernel == FIREX_JACOBI_ZMARCH && zc > 0) ? zc : zm_chunk(zm32, zm16);
-        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 1 : 0))
+        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 1 : 0) ||
+            tableWater != water_signature())
             fill_table(p.k, p.zc, p.zmZc, wantRes);
         p.res = wantRes && resOk;
         if (p.res) {
@@ -703,6 +744,10 @@ struct firex_batch {
         fx_launch_step_begin(stream, d);
         fx_launch_step_tables(stream, d, pl.bricks[FX_SHAPE_TAB]);
         mark(FIREX_PASS_OTHER, 2);
+        if (sph_launches(pl)) {
+            fx_launch_sph(stream, d, pl.bricks[FX_SHAPE_ROW4], pl.bricks[FX_SHAPE_PART]);
+            mark(FIREX_PASS_PARTICLES, sph_launches(pl));
+        }
         fx_launch_simulate(stream, pl.storage, d, pl.bricks[FX_SHAPE_CELL]);
         mark(FIREX_PASS_SIMULATE, 1);
         fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 0);
@@ -758,6 +803,7 @@ struct firex_batch {
                 s->h.dt = dt;
                 s->refresh_params();
             }
+            s->prepare_particles(stream);
             s->flush(stream);
         }
         const StepPlan pl = plan();
@@ -785,6 +831,7 @@ struct firex_batch {
                 pendingLaunches[FIREX_PASS_DIVERGENCE] += 2;
                 pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
                 pendingLaunches[FIREX_PASS_PROJECT] += 2;
+                pendingLaunches[FIREX_PASS_PARTICLES] += sph_launches(pl);
             }
         }
         e = cudaGetLastError();
@@ -857,9 +904,67 @@ int firex_sim::reset() {
     cudaMemsetAsync(h.reaction, 0, (size_t)N * 4, st);
     cudaMemsetAsync(h.liquid, 0, (size_t)N * 4, st);
     fx_launch_init(st, storage, d, 300.0f, (float)named[param_slot("oxygenRate")], opt.velocity_noise);
+    if (h.np > 0) {  // initializeFields (FireXEngine.ts:1972-1973)
+        write_particle_initial_state(st, water_active());
+        liquidMayContainWater = false;
+        h.water = 0;
+        dirty = true;
+        flush(st);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "reset");
     return FIREX_OK;
+}
+
+void firex_sim::write_particle_initial_state(cudaStream_t st, bool active) {
+    const int n = h.np;
+    auto P = [&](const char* k) { return named[param_slot(k)]; };
+    const double domainWidth = P("domainWidth"), domainHeight = P("domainHeight"), domainDepth = P("domainDepth");
+    const double aimX = (0.52 - 0.035) * domainWidth;
+    const double aimY = (P("aimHeight") - 0.5) * domainHeight;
+    const double aimLength = std::hypot(aimX, aimY);
+    const double base[3] = {aimX / aimLength, aimY / aimLength, 0.0};
+    const double tangent[3] = {base[1], -base[0], 0.0};
+    auto hash = [](double v) {
+        const double x = std::sin(v * 12.9898 + 1.317) * 43758.5453;
+        return x - std::floor(x);
+    };
+    const double nozzle = P("nozzleType"), waterFlow = P("waterFlow"), sprayAngle = P("sprayAngle");
+    cudaStreamSynchronize(st);  // the staging buffer may still feed an earlier copy
+    hostParticles.assign((size_t)n * 8, 0.0f);
+    for (int i = 0; i < n; ++i) {
+        float* o = hostParticles.data() + 8 * (size_t)i;
+        const double phase = (double)i / n;
+        const double angle = hash(i * 3.771 + 4.91) * M_PI * 2;
+        const double radial = std::sqrt(hash(i * 3.771 + 0.17));
+        const double spreadScale = nozzle >= 0.5 ? 0.72 : 0.1;
+        const double cone = std::tan((sprayAngle * M_PI) / 180) * radial * spreadScale;
+        const double diskX = tangent[0] * std::cos(angle), diskY = tangent[1] * std::cos(angle), diskZ = -std::sin(angle);
+        double dx = base[0] + diskX * cone, dy = base[1] + diskY * cone, dz = diskZ * cone;
+        const double dl = std::sqrt(dx * dx + dy * dy + dz * dz);
+        dx /= dl;
+        dy /= dl;
+        dz /= dl;
+        const double sv = nozzle >= 0.5 ? 0.24 : 0.05;
+        const double speed = (0.82 + waterFlow * 0.82) * (1 - sv * 0.5 + hash(i * 3.771 + 9.37) * sv);
+        const double age = phase * 0.72;
+        const double originRadius = nozzle >= 0.5 ? 0.006 : 0.0028;
+        o[0] = (float)(0.035 + (diskX * radial * originRadius + dx * speed * age) / domainWidth);
+        o[1] = (float)std::max(0.012, 0.5 + (diskY * radial * originRadius + dy * speed * age - 0.29 * age * age) / domainHeight);
+        o[2] = (float)(0.5 + (diskZ * radial * originRadius + dz * speed * age) / domainDepth);
+        o[3] = (float)(active ? age : -phase * 0.72);
+        o[4] = (float)(active ? dx * speed : 0.0);
+        o[5] = (float)(active ? dy * speed - 0.58 * age : 0.0);
+        o[6] = (float)(active ? dz * speed : 0.0);
+        o[7] = (float)(active ? 0.52 + waterFlow * 0.88 : 0.0);
+    }
+    cudaMemcpyAsync(h.part[0], hostParticles.data(), (size_t)n * 32, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(h.part[1], hostParticles.data(), (size_t)n * 32, cudaMemcpyHostToDevice, st);
+    if (h.pti != 0) {
+        h.pti = 0;
+        dirty = true;
+    }
+    particleFieldActive = active;
 }
 
 void firex_sim::release() {
@@ -918,6 +1023,7 @@ void firex_default_options(firex_options* o) {
     o->correction_iterations = 64;
     o->emitter_mode = FIREX_EMITTER_BURNER;
     o->cinematic = 1;
+    o->particle_count = 640;  // the reference's balanced quality tier (FireXEngine.ts:206)
 }
 
 size_t firex_field_element_size(int32_t field) {
@@ -951,7 +1057,7 @@ uint64_t firex_planned_device_bytes(const int32_t dims[3], const firex_options* 
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
     const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
-    return firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode);
+    return firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode, opt ? opt->particle_count : 0);
 }
 
 int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** out) {
@@ -983,7 +1089,7 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
     const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
-    const size_t need = firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode);
+    const size_t need = firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode, opt->particle_count);
     if (opt->memory_budget_bytes && need > opt->memory_budget_bytes) {
         g_create_error = "grid needs " + std::to_string(need) + " device bytes, above the " +
                          std::to_string(opt->memory_budget_bytes) + "-byte budget";
@@ -1049,6 +1155,10 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
          (s->d_partial = (double*)s->alloc(2 * sizeof(double) * (size_t)fx_norm_partial_blocks(N))) &&
          (s->d_norm = (double*)s->alloc(2 * sizeof(double))) && (h.sync = (unsigned*)s->alloc(FX_RES_SYNC_WORDS * 4)) &&
          cudaMemset(h.sync, 0, FX_RES_SYNC_WORDS * 4) == cudaSuccess;
+    h.np = std::max(0, opt->particle_count);
+    if (ok && h.np > 0)
+        ok = (h.part[0] = (float4*)s->alloc((size_t)h.np * 32)) && (h.part[1] = (float4*)s->alloc((size_t)h.np * 32)) &&
+             (h.pdens = (float4*)s->alloc((size_t)h.np * 16));
     if (!ok) {
         if (g_create_error.empty() || s->solo) g_create_error = "device allocation failed (" + std::to_string(need) + " bytes requested)";
         s->release();
@@ -1257,6 +1367,32 @@ int firex_write_field(firex_sim* s, int32_t field, const void* host, size_t byte
     return FIREX_OK;
 }
 
+int firex_read_particles(firex_sim* s, void* host, size_t bytes) {
+    if (!s || (!host && bytes)) return FIREX_ERR_BAD_ARG;
+    if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
+    if (bytes != (size_t)s->h.np * 32) return s->fail(FIREX_ERR_BAD_ARG, "byte count is not particle_count * 32");
+    if (!bytes) return FIREX_OK;
+    DeviceGuard dg(s->device);
+    cudaStream_t st = s->stream();
+    cudaError_t e = cudaMemcpyAsync(host, s->h.part[s->h.pti], bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "read_particles");
+    return FIREX_OK;
+}
+
+int firex_write_particles(firex_sim* s, const void* host, size_t bytes) {
+    if (!s || (!host && bytes)) return FIREX_ERR_BAD_ARG;
+    if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
+    if (bytes != (size_t)s->h.np * 32) return s->fail(FIREX_ERR_BAD_ARG, "byte count is not particle_count * 32");
+    if (!bytes) return FIREX_OK;
+    DeviceGuard dg(s->device);
+    cudaStream_t st = s->stream();
+    cudaError_t e = cudaMemcpyAsync(s->h.part[s->h.pti], host, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return s->cuda_fail(e, "write_particles");
+    return FIREX_OK;
+}
+
 int firex_divergence_norm(firex_sim* s, double out[3]) {
     if (!s || !out) return FIREX_ERR_BAD_ARG;
     if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier CUDA error");
@@ -1361,7 +1497,8 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_block = p.k;
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
-    out->launches_per_step = 8 + (p.pack ? 1 : 0) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+    out->launches_per_step =
+        8 + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     return FIREX_OK;

@@ -37,6 +37,9 @@ int fx_res_capacity(bool half);
 void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbient, float oxygen, float noise);
 void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask);
 void fx_launch_final_divergence(cudaStream_t s, const FxSimDev* S, float* out);
+// The particle passes of every member whose water runs (liquid clear, density,
+// integration, deposition), before simulate (fx_sph.cuh).
+void fx_launch_sph(cudaStream_t s, const FxBatchDev* B, int rowBricks, int partBricks);
 // Render volumes: one simulation (a read), or every packing member of a batch (step end).
 void fx_launch_pack_sim(cudaStream_t s, const FxSimDev* S);
 void fx_launch_pack_batch(cudaStream_t s, const FxBatchDev* B, int bricks);

@@ -15,6 +15,7 @@
 
 #include "fx_internal.h"
 #include "fx_jacobi_res.cuh"
+#include "fx_sph.cuh"
 #include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
 #include "fx_step_math.cuh"
@@ -57,6 +58,7 @@ __global__ void fxk_step_end(FxBatchDev* __restrict__ B) {
         S->fi ^= 1;
         S->si ^= 1;
         S->pi = (S->mode == FIREX_PRESSURE_COLD_F32) ? (S->P & 1) : (S->pi ^ (S->P & 1));
+        if (S->water) S->pti ^= 1;
     }
 }
 
@@ -419,6 +421,45 @@ __global__ void fxk_emitter_mask(const FxSimDev* __restrict__ S, uint8_t* __rest
     }
 }
 
+// ---- SPH droplets and liquid deposition (fx_sph.cuh), before simulate --------------------
+// Members whose water runs: clear the liquid field, then density, integration (droplets
+// part[pti] -> part[pti ^ 1]) and deposition; step_end flips pti.
+__global__ void __launch_bounds__(256) fxk_sph_clear(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+        if (!S.water) return;
+        const long long i = (long long)b * (FX_ROW4_THREADS * 4) + 4 * threadIdx.x;
+        const long long n = (long long)S.X * S.Y * S.Z;
+        if (i < n) *reinterpret_cast<uint4*>(S.liquid + i) = make_uint4(0u, 0u, 0u, 0u);  // n % 4 == 0
+    });
+}
+__global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_density(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_PART>(B, [&](const FxSimDev& S, int b) {
+        const int i = b * FX_SPH_THREADS + threadIdx.x;
+        if (i >= S.np) return;
+        const fxsph::Ctx c{S.prm.u, S.X, S.Y, S.Z};
+        S.pdens[i] = fxsph::density(c, S.np, S.part[S.pti], i);
+    });
+}
+__global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_integrate(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_PART>(B, [&](const FxSimDev& S, int b) {
+        const int i = b * FX_SPH_THREADS + threadIdx.x;
+        if (i >= S.np) return;
+        const fxsph::Ctx c{S.prm.u, S.X, S.Y, S.Z};
+        float4 oa, om;
+        fxsph::integrate(c, S.np, S.part[S.pti], S.pdens, reinterpret_cast<const float4*>(S.flow[S.fi]), i, oa, om);
+        S.part[S.pti ^ 1][2 * i] = oa;
+        S.part[S.pti ^ 1][2 * i + 1] = om;
+    });
+}
+__global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_deposit(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_PART>(B, [&](const FxSimDev& S, int b) {
+        const int i = b * FX_SPH_THREADS + threadIdx.x;
+        if (i >= S.np) return;
+        const fxsph::Ctx c{S.prm.u, S.X, S.Y, S.Z};
+        fxsph::deposit(c, S.part[S.pti], S.part[S.pti ^ 1], S.liquid, i);
+    });
+}
+
 // ---- render-field packing (storePackedFields, qualityShaders.ts:37-75) --------------------
 // The three rgba16float volumes of the canonical state as FP16 (round to nearest even):
 // flow (u, v, w, clamp((T - 300) / 2600, 0, 1)), chemistry (max(species, 0)) and media
@@ -770,6 +811,14 @@ void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbie
 
 void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask) {
     fxk_emitter_mask<<<num_sms() * 8, 256, 0, s>>>(S, mask);
+}
+
+void fx_launch_sph(cudaStream_t s, const FxBatchDev* B, int rowBricks, int partBricks) {
+    static int g = persistent_grid((const void*)fxk_sph_clear, 256, 1 << 30);
+    fxk_sph_clear<<<row4_grid(g, rowBricks), 256, 0, s>>>(B);
+    fxk_sph_density<<<partBricks, FX_SPH_THREADS, 0, s>>>(B);
+    fxk_sph_integrate<<<partBricks, FX_SPH_THREADS, 0, s>>>(B);
+    fxk_sph_deposit<<<partBricks, FX_SPH_THREADS, 0, s>>>(B);
 }
 
 void fx_launch_pack_sim(cudaStream_t s, const FxSimDev* S) { fxk_pack_sim<<<num_sms() * 8, 256, 0, s>>>(S); }

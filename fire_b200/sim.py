@@ -57,6 +57,7 @@ def make_options(
     cinematic: bool = True,
     jacobi_block: int = 0,
     memory_budget_bytes: int = 0,
+    particle_count: int = 640,
 ) -> A.Options:
     """Options with the library defaults (firex_default_options) plus overrides.
 
@@ -86,6 +87,7 @@ def make_options(
     o.cinematic = 1 if cinematic else 0
     o.jacobi_block = jacobi_block
     o.memory_budget_bytes = memory_budget_bytes
+    o.particle_count = particle_count
     return o
 
 
@@ -178,6 +180,21 @@ class _Handle:
         dtype, shape = self._shape(f)
         arr = np.ascontiguousarray(data, dtype=dtype).reshape(shape)
         self._check(self._fn("write_field")(self._h, f, arr.ctypes.data_as(C.c_void_p), arr.nbytes))
+
+    # -- droplets ----------------------------------------------------------------------------
+    @property
+    def particle_count(self) -> int:
+        return int(self.options.particle_count)
+
+    def read_particles(self) -> np.ndarray:
+        """Droplets as (particle_count, 2, 4) float32: (x, y, z, age), (vx, vy, vz, mass)."""
+        out = np.empty((self.particle_count, 2, 4), dtype=np.float32)
+        self._check(self._fn("read_particles")(self._h, out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def write_particles(self, data: np.ndarray) -> None:
+        arr = np.ascontiguousarray(data, dtype=np.float32).reshape(self.particle_count, 2, 4)
+        self._check(self._fn("write_particles")(self._h, arr.ctypes.data_as(C.c_void_p), arr.nbytes))
 
     def divergence_norm(self) -> tuple[float, float, int]:
         out = (C.c_double * 3)()

@@ -87,7 +87,9 @@ typedef struct firex_options {
     int32_t jacobi_block;          /* > 1: fuse this many Jacobi sweeps per launch (see firex_set_jacobi) */
     uint64_t memory_budget_bytes;  /* 0 = no budget; else create fails with FIREX_ERR_BUDGET */
     int32_t jacobi_zchunk;         /* z planes per CTA of a fused Jacobi launch; 0 = auto */
-    int32_t reserved[7];
+    int32_t particle_count;        /* SPH droplets (FIREX_QUALITY particleCount, FireXEngine.ts:187-277);
+                                      they run while waterEnabled and waterFlow > 0.001 */
+    int32_t reserved[6];
 } firex_options;
 
 /* Fills *opt with the defaults: F32, AUTO pressure, P = R = 64 (offline HD tier,
@@ -191,6 +193,14 @@ int firex_read_field_async(firex_sim* sim, int32_t field, void* host, size_t byt
 int firex_set_render_packing(firex_sim* sim, int32_t on);
 int firex_render_volumes(const firex_sim* sim, void* out[3]);
 
+/* SPH droplets (particleBuffers, FireXEngine.ts:1598-1603): particle_count records of
+ * two float4 each, (x, y, z, age) in domain units [0,1] and (vx, vy, vz, mass), as the
+ * droplets stand after the steps so far. bytes must equal particle_count * 32. A write
+ * replaces the current droplet state (the next step reads it); it does not change
+ * whether the spray is on: that follows waterEnabled and waterFlow at every step. */
+int firex_read_particles(firex_sim* sim, void* host, size_t bytes);
+int firex_write_particles(firex_sim* sim, const void* host, size_t bytes);
+
 /* Post-projection divergence of FLOW over interior cells (the one-cell outer shell is
  * excluded, qualityShaders.ts:47-57), reduced in FP64: out[0] = L2 norm, out[1] = max
  * abs, out[2] = number of interior cells. (Presentation diagnostic, FireXEngine.ts:2588-2596.) */
@@ -247,7 +257,8 @@ void* firex_stream(const firex_sim* sim);
 #define FIREX_PASS_JACOBI 2     /* every primary and residual Jacobi launch */
 #define FIREX_PASS_PROJECT 3    /* both projections */
 #define FIREX_PASS_OTHER 4      /* parameter upload and buffer clears */
-#define FIREX_PASS_COUNT 5
+#define FIREX_PASS_PARTICLES 5  /* droplet pass: liquid clear, density, integrate, deposit */
+#define FIREX_PASS_COUNT 6
 
 /* Turns per-pass event recording on (1) or off (0) for subsequent steps. */
 int firex_set_profiling(firex_sim* sim, int32_t on);

@@ -32,6 +32,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #ifdef _OPENMP
@@ -223,17 +224,17 @@ static bool get_named(const Named& p, const std::string& n, double* v) {
 }
 
 // writeUniforms (FireXEngine.ts:2043-2113): the 44-float block. Presentation-only entries
-// (canvas aspect and size, ray steps, particle count) are written as 1, 1, 1, 0, 0: the
-// step does not read them.
+// (canvas aspect and size, ray steps) are written as 1, 1, 1, 0: the step does not read
+// them; render.w is the particle count (:2069), which the particle passes read.
 static void write_uniforms(float out[44], const Named& p, int X, int Y, int Z, double dt, double simTime,
-                           int64_t frameIndex, int cinematic) {
+                           int64_t frameIndex, int cinematic, int particles = 0) {
     double cells = (double)X * (double)Y * (double)Z;
     double v[44] = {(double)X, (double)Y, (double)Z, cells,
                     (double)dt, simTime, (double)frameIndex, (double)dt,
                     p.fuelRate, p.oxygenRate, p.heatEfficiency, p.vorticity,
                     p.waterFlow, (p.sprayAngle * M_PI) / 180, p.waterEnabled ? 1.0 : 0.0, 300,
                     p.cameraYaw, p.cameraPitch, p.cameraDistance, 1,
-                    1, 1, 0, 0,
+                    1, 1, 0, (double)particles,
                     p.viewMode, p.aimHeight, p.nozzleType, p.exposure,
                     p.burnerSize, p.burnerDepth, p.sourceThickness, p.firePower,
                     p.domainWidth, p.domainHeight, p.domainDepth, 0,
@@ -628,6 +629,297 @@ static void simulate_pass(const Grid<T>& g, const V4<T>* flowIn, const V4<T>* sp
 }
 
 // ---------------------------------------------------------------------------------------
+// SPH droplets and liquid deposition (FIREX_PARTICLE_WGSL, shaders.ts:514-825), in f32 as
+// the reference. A particle is 8 floats: position (domain-normalised), age, velocity, mass.
+// sin, cos, tan and exp are evaluated in double and rounded to float (the CUDA path does
+// the same): the hash fract(sin(x) * 43758.5453) amplifies one ulp of sin into 1e-3, so
+// the two sides must agree on those to agree on the droplets.
+namespace sph {
+static inline float sinF(float x) { return (float)std::sin((double)x); }
+static inline float cosF(float x) { return (float)std::cos((double)x); }
+static inline float tanF(float x) { return (float)std::tan((double)x); }
+static inline float expF(float x) { return (float)std::exp((double)x); }
+static inline float fract(float x) { return x - std::floor(x); }
+static inline float hash11(float v) { return fract(sinF(v * 12.9898f + 1.317f) * 43758.5453f); }
+struct F3 {
+    float x, y, z;
+};
+static inline F3 add(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+static inline F3 sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline F3 mul(F3 a, F3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+static inline F3 muls(F3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+static inline F3 divv(F3 a, F3 b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
+static inline F3 divs(F3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+static inline float len(F3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+static inline F3 norm(F3 a) { return divs(a, len(a)); }
+static inline F3 cross(F3 a, F3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+static inline float maxf(float a, float b) { return a < b ? b : a; }
+static inline float minf(float a, float b) { return b < a ? b : a; }
+static inline float clampf(float x, float lo, float hi) { return minf(maxf(x, lo), hi); }
+static inline float smoothstepf(float e0, float e1, float x) {
+    float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+static inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+
+struct Ctx {
+    const float* u;  // uniform block
+    int X, Y, Z;
+    F3 ext() const { return {maxf(u[32], 0.001f), maxf(u[33], 0.001f), maxf(u[34], 0.001f)}; }
+    bool spray() const { return u[26] >= 0.5f; }  // controls.z: nozzle type
+};
+static inline F3 nozzleOrigin() { return {0.035f, 0.50f, 0.5f}; }
+static inline F3 nozzleDirection(const Ctx& c) {
+    const F3 target = {0.52f, clampf(c.u[25], 0.08f, 0.82f), 0.5f};
+    return norm(mul(sub(target, nozzleOrigin()), c.ext()));
+}
+// spawnParticle (shaders.ts:575-600)
+static inline void spawn(const Ctx& c, unsigned id, float cycle, float* out) {
+    const float seed = (float)id * 3.771f + cycle * 19.173f;
+    const float radialRandom = std::sqrt(hash11(seed + 0.17f));
+    const float angularRandom = hash11(seed + 4.91f) * 6.2831853f;
+    const float speedRandom = hash11(seed + 9.37f);
+    const F3 direction = nozzleDirection(c);
+    const F3 tangent = norm(cross(direction, {0.0f, 0.0f, 1.0f}));
+    const F3 bitangent = norm(cross(direction, tangent));
+    const F3 disk = add(muls(tangent, cosF(angularRandom)), muls(bitangent, sinF(angularRandom)));
+    const float spread = c.spray() ? 0.72f : 0.10f;
+    const float cone = tanF(clampf(c.u[13], 0.005f, 0.78f)) * radialRandom * spread;
+    const F3 launch = norm(add(direction, muls(disk, cone)));
+    const float originRadius = c.spray() ? 0.006f : 0.0028f;
+    const F3 origin = add(nozzleOrigin(), divv(muls(muls(disk, radialRandom), originRadius), c.ext()));
+    const float sv = c.spray() ? 0.24f : 0.05f;
+    const float speed = (0.82f + c.u[12] * 0.82f) * mixf(1.0f - sv * 0.5f, 1.0f + sv * 0.5f, speedRandom);
+    out[0] = origin.x, out[1] = origin.y, out[2] = origin.z, out[3] = 0.0f;
+    const F3 v = muls(launch, speed);
+    out[4] = v.x, out[5] = v.y, out[6] = v.z, out[7] = 0.52f + c.u[12] * 0.88f;
+}
+static inline size_t cellIndex(const Ctx& c, int x, int y, int z) {
+    x = std::min(std::max(x, 0), c.X - 1);
+    y = std::min(std::max(y, 0), c.Y - 1);
+    z = std::min(std::max(z, 0), c.Z - 1);
+    return (size_t)x + (size_t)c.X * ((size_t)y + (size_t)c.Y * z);
+}
+// computeParticleDensity (shaders.ts:602-638)
+static void density(const Ctx& c, int n, const float* pin, float* dens) {
+    const F3 ext = c.ext();
+    const float r = c.spray() ? 0.060f : 0.038f;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        const float* p = pin + 8 * i;
+        float* d = dens + 4 * i;
+        if (p[7] <= 0.0001f) {
+            d[0] = d[1] = d[2] = d[3] = 0.0f;
+            continue;
+        }
+        float de = 0.0f, near = 0.0f;
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const float* q = pin + 8 * j;
+            if (q[7] <= 0.0001f) continue;
+            const float dist = len(mul(sub({p[0], p[1], p[2]}, {q[0], q[1], q[2]}), ext));
+            if (dist > 0.00001f && dist < r) {
+                const float w = 1.0f - dist / r;
+                de += w * w;
+                near += w * w * w;
+            }
+        }
+        const float rest = 2.7f + c.u[12] * 0.9f;
+        d[0] = de, d[1] = near, d[2] = maxf(de - rest, 0.0f) * 0.055f, d[3] = near * 0.065f;
+    }
+}
+// integrateParticles (shaders.ts:640-736); flow: the canonical flow field, as float4
+static void integrate(const Ctx& c, int n, const float* pin, const float* dens, const float* flow, float* pout) {
+    const F3 ext = c.ext();
+    const float dt = c.u[4];
+    const bool waterOn = c.u[14] >= 0.5f && c.u[12] > 0.001f;
+    const float r = c.spray() ? 0.060f : 0.038f;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        const float* p = pin + 8 * i;
+        float* o = pout + 8 * i;
+        if (dt <= 0.0f) {
+            std::memcpy(o, p, 32);
+            continue;
+        }
+        if (p[7] <= 0.0001f) {
+            const float wait = p[3] + dt;
+            if (waterOn && wait >= 0.0f) {
+                spawn(c, (unsigned)i, wait + c.u[6], o);
+            } else {
+                const F3 no = nozzleOrigin();
+                o[0] = no.x, o[1] = no.y, o[2] = no.z, o[3] = wait > 0.0f ? -0.72f : wait;
+                o[4] = o[5] = o[6] = o[7] = 0.0f;
+            }
+            continue;
+        }
+        const float lifetime = 0.88f + hash11((float)i * 2.31f + 7.0f) * 0.52f;
+        const float nextAge = p[3] + dt;
+        const bool outside = p[0] < -0.03f || p[1] < -0.03f || p[2] < -0.03f || p[0] > 1.03f || p[1] > 1.03f || p[2] > 1.03f;
+        if (nextAge >= lifetime || outside) {
+            if (waterOn) {
+                spawn(c, (unsigned)i, nextAge + c.u[6], o);
+            } else {
+                const F3 no = nozzleOrigin();
+                o[0] = no.x, o[1] = no.y, o[2] = no.z, o[3] = -hash11((float)i * 8.17f) * 0.72f;
+                o[4] = o[5] = o[6] = o[7] = 0.0f;
+            }
+            continue;
+        }
+        const F3 pos = {p[0], p[1], p[2]};
+        F3 vel = {p[4], p[5], p[6]};
+        const float* pd = dens + 4 * i;
+        F3 pa = {0, 0, 0}, va = {0, 0, 0};
+        for (int j = 0; j < n; ++j) {
+            if (j == i) continue;
+            const float* q = pin + 8 * j;
+            if (q[7] <= 0.0001f) continue;
+            const F3 sep = mul(sub(pos, {q[0], q[1], q[2]}), ext);
+            const float dist = len(sep);
+            if (dist > 0.00001f && dist < r) {
+                const float w = 1.0f - dist / r;
+                const F3 dir = divs(sep, dist);
+                const float* nd = dens + 4 * j;
+                const float pr = (pd[2] + nd[2]) * w;
+                const float npr = (pd[3] + nd[3]) * w * w;
+                pa = add(pa, muls(dir, pr + npr));
+                va = add(va, muls(sub({q[4], q[5], q[6]}, vel), w * 0.018f));
+            }
+        }
+        // sampleFlow: nearest cell of the canonical flow
+        const int cx = (int)(clampf(pos.x, 0.0f, 0.99999f) * c.u[0]);
+        const int cy = (int)(clampf(pos.y, 0.0f, 0.99999f) * c.u[1]);
+        const int cz = (int)(clampf(pos.z, 0.0f, 0.99999f) * c.u[2]);
+        const float* g = flow + 4 * cellIndex(c, cx, cy, cz);
+        const float heat = smoothstepf(380.0f, 1500.0f, g[3]);
+        F3 acc = {0.0f, -0.58f, 0.0f};
+        acc = add(acc, muls(sub({g[0], g[1], g[2]}, vel), 0.30f + heat * 0.18f));
+        const float disp = c.spray() ? 1.0f : 0.055f;
+        const float coh = c.spray() ? 1.0f : 2.2f;
+        acc = add(acc, add(muls(pa, disp), muls(va, coh)));
+        vel = add(vel, muls(acc, dt));
+        F3 next = add(pos, divv(muls(vel, dt), ext));
+        if (next.y < 0.012f) {
+            next.y = 0.012f;
+            vel.y = std::fabs(vel.y) * 0.18f;
+            vel = {vel.x * 0.72f, vel.y, vel.z * 0.72f};
+        }
+        if (next.x < 0.008f || next.x > 0.992f) {
+            next.x = clampf(next.x, 0.008f, 0.992f);
+            vel.x *= -0.24f;
+        }
+        if (next.z < 0.008f || next.z > 0.992f) {
+            next.z = clampf(next.z, 0.008f, 0.992f);
+            vel.z *= -0.24f;
+        }
+        const float mass = p[7] * expF(-heat * dt * 0.34f);
+        o[0] = next.x, o[1] = next.y, o[2] = next.z, o[3] = nextAge;
+        o[4] = clampf(vel.x, -2.0f, 2.0f), o[5] = clampf(vel.y, -2.0f, 2.0f), o[6] = clampf(vel.z, -2.0f, 2.0f);
+        o[7] = mass;
+    }
+}
+// depositParticles (shaders.ts:738-824): 16.12 fixed-point liquid mass, integer sums
+static inline void corner(const Ctx& c, uint32_t* liq, int x, int y, int z, float weight, float mass) {
+    const uint32_t fixed = (uint32_t)clampf(weight * mass * 4096.0f, 0.0f, 65535.0f);
+    liq[cellIndex(c, x, y, z)] += fixed;
+}
+static void deposit_at(const Ctx& c, uint32_t* liq, F3 position, float mass) {
+    const F3 vp = sub(mul(position, {c.u[0], c.u[1], c.u[2]}), {0.5f, 0.5f, 0.5f});
+    if (!c.spray()) {
+        const int bx = (int)std::floor(vp.x), by = (int)std::floor(vp.y), bz = (int)std::floor(vp.z);
+        const F3 f = {fract(vp.x), fract(vp.y), fract(vp.z)};
+        const F3 iv = {1.0f - f.x, 1.0f - f.y, 1.0f - f.z};
+        const float m = mass * 0.20f;
+        corner(c, liq, bx, by, bz, iv.x * iv.y * iv.z, m);
+        corner(c, liq, bx + 1, by, bz, f.x * iv.y * iv.z, m);
+        corner(c, liq, bx, by + 1, bz, iv.x * f.y * iv.z, m);
+        corner(c, liq, bx + 1, by + 1, bz, f.x * f.y * iv.z, m);
+        corner(c, liq, bx, by, bz + 1, iv.x * iv.y * f.z, m);
+        corner(c, liq, bx + 1, by, bz + 1, f.x * iv.y * f.z, m);
+        corner(c, liq, bx, by + 1, bz + 1, iv.x * f.y * f.z, m);
+        corner(c, liq, bx + 1, by + 1, bz + 1, f.x * f.y * f.z, m);
+        return;
+    }
+    const int cx = (int)std::nearbyint(vp.x), cy = (int)std::nearbyint(vp.y), cz = (int)std::nearbyint(vp.z);
+    float total = 0.0f;
+    for (int oz = -1; oz <= 1; ++oz)
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                const float d = len(sub(vp, {(float)(cx + ox), (float)(cy + oy), (float)(cz + oz)}));
+                const float k = maxf(0.0f, 1.0f - d * 0.52f);
+                total += k * k;
+            }
+    for (int oz = -1; oz <= 1; ++oz)
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                const float d = len(sub(vp, {(float)(cx + ox), (float)(cy + oy), (float)(cz + oz)}));
+                const float k = maxf(0.0f, 1.0f - d * 0.52f);
+                corner(c, liq, cx + ox, cy + oy, cz + oz, k * k / maxf(total, 0.0001f), mass);
+            }
+}
+static void deposit(const Ctx& c, int n, const float* pin, const float* pout, uint32_t* liq) {
+    const F3 ext = c.ext();
+    for (int i = 0; i < n; ++i) {
+        const float* o = pout + 8 * i;
+        const F3 pos = {o[0], o[1], o[2]};
+        const float mass = o[7];
+        if (mass <= 0.0001f || pos.x < 0.0f || pos.y < 0.0f || pos.z < 0.0f || pos.x >= 1.0f || pos.y >= 1.0f ||
+            pos.z >= 1.0f)
+            continue;
+        const float* p = pin + 8 * i;
+        const F3 disp = sub(pos, {p[0], p[1], p[2]});
+        const bool sweep = p[7] > 0.0001f && o[3] >= p[3] && len(mul(disp, ext)) < 0.20f;
+        if (!sweep) {
+            deposit_at(c, liq, pos, mass);
+            continue;
+        }
+        for (unsigned k = 0; k < 3u; ++k) {
+            const float fr = (float)k / 2.0f;
+            deposit_at(c, liq, add({p[0], p[1], p[2]}, muls(disp, fr)), mass / 3.0f);
+        }
+    }
+}
+// writeParticleInitialState (FireXEngine.ts:1976-2034): host double arithmetic, stored f32
+static void initial_state(const Named& nm, int n, bool active, float* out) {
+    const double aimX = (0.52 - 0.035) * nm.domainWidth;
+    const double aimY = (nm.aimHeight - 0.5) * nm.domainHeight;
+    const double aimLength = std::hypot(aimX, aimY);
+    const double base[3] = {aimX / aimLength, aimY / aimLength, 0.0};
+    const double tangent[3] = {base[1], -base[0], 0.0};
+    auto hash = [](double v) {
+        const double h = std::sin(v * 12.9898 + 1.317) * 43758.5453;
+        return h - std::floor(h);
+    };
+    for (int i = 0; i < n; ++i) {
+        float* o = out + 8 * i;
+        const double phase = (double)i / n;
+        const double angle = hash(i * 3.771 + 4.91) * M_PI * 2;
+        const double radial = std::sqrt(hash(i * 3.771 + 0.17));
+        const double spreadScale = nm.nozzleType >= 0.5 ? 0.72 : 0.1;
+        const double cone = std::tan((nm.sprayAngle * M_PI) / 180) * radial * spreadScale;
+        const double diskX = tangent[0] * std::cos(angle), diskY = tangent[1] * std::cos(angle), diskZ = -std::sin(angle);
+        double dx = base[0] + diskX * cone, dy = base[1] + diskY * cone, dz = diskZ * cone;
+        const double dl = std::sqrt(dx * dx + dy * dy + dz * dz);
+        dx /= dl;
+        dy /= dl;
+        dz /= dl;
+        const double sv = nm.nozzleType >= 0.5 ? 0.24 : 0.05;
+        const double speed = (0.82 + nm.waterFlow * 0.82) * (1 - sv * 0.5 + hash(i * 3.771 + 9.37) * sv);
+        const double age = phase * 0.72;
+        const double originRadius = nm.nozzleType >= 0.5 ? 0.006 : 0.0028;
+        o[0] = (float)(0.035 + (diskX * radial * originRadius + dx * speed * age) / nm.domainWidth);
+        o[1] = (float)std::max(0.012, 0.5 + (diskY * radial * originRadius + dy * speed * age - 0.29 * age * age) / nm.domainHeight);
+        o[2] = (float)(0.5 + (diskZ * radial * originRadius + dz * speed * age) / nm.domainDepth);
+        o[3] = (float)(active ? age : -phase * 0.72);
+        o[4] = (float)(active ? dx * speed : 0.0);
+        o[5] = (float)(active ? dy * speed - 0.58 * age : 0.0);
+        o[6] = (float)(active ? dz * speed : 0.0);
+        o[7] = (float)(active ? 0.52 + nm.waterFlow * 0.88 : 0.0);
+    }
+}
+}  // namespace sph
+
+// ---------------------------------------------------------------------------------------
 // The engine: resources (FireXEngine.ts:1573-1603), initializeFields (:1933-1974),
 // encodeSimulationStep (:2115-2276).
 struct SimBase {
@@ -650,6 +942,19 @@ struct SimBase {
     // interior cells: L2, max abs, cell count. The accuracy metric of mixed precision
     // normalises divergence differences by this L2 norm of the FP64 step.
     double preDiv[3] = {0, 0, 0};
+    // particles (8 floats each, ping-pong) and their density (4 floats each)
+    int np = 0;
+    std::vector<float> particles[2], pdensity;
+    int particleIndex = 0;
+    bool particleFieldActive = false, liquidMayContainWater = false;
+    bool water_active() const { return named.waterEnabled && named.waterFlow > 0.001; }
+    void write_particle_initial_state(bool active) {
+        particles[0].assign((size_t)np * 8, 0.0f);
+        sph::initial_state(named, np, active, particles[0].data());
+        particles[1] = particles[0];
+        particleIndex = 0;
+        particleFieldActive = active;
+    }
 };
 
 template <typename T>
@@ -685,7 +990,7 @@ struct Sim : SimBase {
         g.Z = Z;
         g.N = N;
         float u[44];
-        write_uniforms(u, named, X, Y, Z, dt, simulationTime, frameIndex, opt.cinematic);
+        write_uniforms(u, named, X, Y, Z, dt, simulationTime, frameIndex, opt.cinematic, np);
         for (int i = 0; i < 44; ++i) g.u[i] = T(u[i]);
         g.ext.emitterMode = opt.emitter_mode;
         g.ext.numSpheres = opt.num_spheres;
@@ -695,6 +1000,9 @@ struct Sim : SimBase {
     }
 
     void reset() override {
+        pdensity.assign((size_t)np * 4, 0.0f);
+        write_particle_initial_state(water_active());  // initializeFields (FireXEngine.ts:1972-1973)
+        liquidMayContainWater = false;
         simulationTime = 0;
         frameIndex = 0;
         speciesIndex = 0;
@@ -718,8 +1026,44 @@ struct Sim : SimBase {
         }
     }
 
+    // The particle passes that precede simulate (FireXEngine.ts:2158-2171): droplets move
+    // and deposit into the liquid field while water runs; when it stops, the liquid field is
+    // cleared and the droplets return to their inactive initial state.
+    void particle_pass(const Grid<T>& g) {
+        if (water_active()) {
+            if (!particleFieldActive) write_particle_initial_state(true);
+            std::fill(liquid.begin(), liquid.end(), 0u);
+            float u[44];
+            for (int i = 0; i < 44; ++i) u[i] = (float)g.u[i];
+            const sph::Ctx c{u, X, Y, Z};
+            std::vector<float> conv;
+            const float* flowf;
+            if (std::is_same<T, float>::value) {
+                flowf = reinterpret_cast<const float*>(flow[0].data());
+            } else {
+                conv.resize(N * 4);
+                for (size_t i = 0; i < N; ++i) {
+                    conv[4 * i] = (float)flow[0][i].x, conv[4 * i + 1] = (float)flow[0][i].y;
+                    conv[4 * i + 2] = (float)flow[0][i].z, conv[4 * i + 3] = (float)flow[0][i].w;
+                }
+                flowf = conv.data();
+            }
+            const int pi = particleIndex;
+            sph::density(c, np, particles[pi].data(), pdensity.data());
+            sph::integrate(c, np, particles[pi].data(), pdensity.data(), flowf, particles[1 - pi].data());
+            sph::deposit(c, np, particles[pi].data(), particles[1 - pi].data(), liquid.data());
+            particleIndex = 1 - pi;
+            liquidMayContainWater = true;
+        } else if (liquidMayContainWater || particleFieldActive) {
+            std::fill(liquid.begin(), liquid.end(), 0u);
+            write_particle_initial_state(false);
+            liquidMayContainWater = false;
+        }
+    }
+
     void step(double dt) override {
         Grid<T> g = grid(dt);
+        particle_pass(g);
         int s = speciesIndex;
         simulate_pass(g, flow[0].data(), species[s].data(), liquid.data(), flow[1].data(), species[1 - s].data(),
                       reaction.data());
@@ -867,7 +1211,7 @@ struct Sim : SimBase {
     // presentation computes from flow[0] (FireXEngine.ts:2588-2596), 0 on the outer shell.
     void render_pack(int which, uint16_t* out) {
         float u[44];
-        write_uniforms(u, named, X, Y, Z, 0.0, simulationTime, frameIndex, opt.cinematic);
+        write_uniforms(u, named, X, Y, Z, 0.0, simulationTime, frameIndex, opt.cinematic, np);
         const bool view7 = (unsigned)clampT(std::nearbyint(u[24]), 0.0f, 7.0f) == 7u;
         std::vector<T> d;
         if (view7) {
@@ -1004,6 +1348,7 @@ int fxo_create(int precision, const int32_t dims[3], const firex_options* opt, v
     s->Z = dims[2];
     s->N = (size_t)dims[0] * dims[1] * dims[2];
     s->opt = *opt;
+    s->np = std::max(0, opt->particle_count);
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO)
         mode = ((long long)s->N >= FIREX_HEAVY_GRID_CELL_THRESHOLD) ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
@@ -1069,7 +1414,7 @@ int fxo_set_state(void* h, const firex_state* st) {
 
 int fxo_get_uniforms(void* h, double dt, float out[44]) {
     SimBase* s = (SimBase*)h;
-    write_uniforms(out, s->named, s->X, s->Y, s->Z, dt, s->simulationTime, s->frameIndex, s->opt.cinematic);
+    write_uniforms(out, s->named, s->X, s->Y, s->Z, dt, s->simulationTime, s->frameIndex, s->opt.cinematic, s->np);
     return FIREX_OK;
 }
 
@@ -1079,6 +1424,20 @@ int fxo_divergence_norm(void* h, double out[3]) {
 }
 
 int fxo_pressure_mode(void* h) { return ((SimBase*)h)->mode; }
+
+// The current droplets (8 floats each: position, age, velocity, mass).
+int fxo_read_particles(void* h, void* out, size_t bytes) {
+    SimBase* s = (SimBase*)h;
+    if (bytes != (size_t)s->np * 32) return FIREX_ERR_BAD_ARG;
+    if (bytes) std::memcpy(out, s->particles[s->particleIndex].data(), bytes);
+    return FIREX_OK;
+}
+int fxo_write_particles(void* h, const void* in, size_t bytes) {
+    SimBase* s = (SimBase*)h;
+    if (bytes != (size_t)s->np * 32) return FIREX_ERR_BAD_ARG;
+    if (bytes) std::memcpy(s->particles[s->particleIndex].data(), in, bytes);
+    return FIREX_OK;
+}
 
 int fxo_pre_projection_norm(void* h, double out[3]) {
     for (int i = 0; i < 3; ++i) out[i] = ((SimBase*)h)->preDiv[i];

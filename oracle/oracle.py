@@ -54,6 +54,8 @@ def load() -> C.CDLL:
             "fxo_divergence_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
             "fxo_pressure_mode": (C.c_int, [vp]),
             "fxo_pre_projection_norm": (C.c_int, [vp, C.POINTER(C.c_double)]),
+            "fxo_read_particles": (C.c_int, [vp, vp, C.c_size_t]),
+            "fxo_write_particles": (C.c_int, [vp, vp, C.c_size_t]),
             "fxo_emission_jitter": (C.c_float, [C.c_uint64, C.c_int64, C.c_float]),
             "fxo_velocity_noise": (C.c_float, [C.c_uint64, C.c_uint64, C.c_int, C.c_float]),
             "fxo_f32_to_f16": (C.c_uint16, [C.c_float]),

@@ -28,8 +28,21 @@ CASES = {
     "burner_warm_f32": dict(options=lambda: burner_options(P=8, R=6), steps=3),
     "spheres_f16_pressure": dict(options=lambda: sphere_options(DIMS, P=8, R=6, pressure_mode=A.PRESSURE_F16), steps=3),
     "spheres_cold_f32": dict(options=lambda: sphere_options(DIMS, P=8, R=6, pressure_mode=A.PRESSURE_COLD_F32), steps=3),
+    # the hose on (full-cone nozzle, 25 degrees): droplets, their liquid deposit and its cooling
+    "spheres_water": dict(options=lambda: sphere_options(DIMS, P=8, R=6, particle_count=384), steps=3,
+                          params={"waterEnabled": True, "waterFlow": 0.8, "nozzleType": 1, "sprayAngle": 25}),
 }
-FIELDS = ("flow", "species", "pressure", "reaction", "divergence", "correction")
+FIELDS = ("flow", "species", "pressure", "reaction", "divergence", "correction", "liquid")
+
+
+def start(sim, case):
+    """Applies a case's parameters to a new simulation and re-initialises it under them."""
+    params = case.get("params")
+    if params:
+        for k, v in params.items():
+            sim.set_parameter(k, v)
+        sim.reset()
+    return sim
 
 
 def generate():
@@ -38,10 +51,11 @@ def generate():
     arrays = {}
     for name, case in CASES.items():
         for precision in (32, 64):
-            sim = O.OracleSim(DIMS, case["options"](), precision=precision)
+            sim = start(O.OracleSim(DIMS, case["options"](), precision=precision), case)
             sim.step(case["steps"], DT)
             for f in FIELDS:
                 arrays[f"{name}/fp{precision}/{f}"] = sim.read(f)
+            arrays[f"{name}/fp{precision}/particles"] = sim.read_particles()
             meta["cases"][f"{name}/fp{precision}"] = {"steps": case["steps"], "divergence_norm": list(sim.divergence_norm()),
                                                       "state": sim.state}
             sim.close()

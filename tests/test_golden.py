@@ -12,7 +12,7 @@ import pytest
 
 from fire_b200.sim import FireXSim
 from oracle.oracle import OracleSim
-from tests.golden.make_golden import CASES, DIMS, FIELDS
+from tests.golden.make_golden import CASES, DIMS, FIELDS, start
 from tests.helpers import DT, max_abs
 
 HERE = Path(__file__).resolve().parent / "golden"
@@ -22,16 +22,19 @@ META = json.loads((HERE / "oracle_step_8x12x8.json").read_text())
 # max-abs bounds on the GPU against the FP32 oracle after 3 steps (dt = 1/60); pressure,
 # correction and divergence relative to the field's max magnitude
 ATOL = {"flow": 2e-3, "species": 2e-5, "reaction": 2e-5}
-REL = {"pressure": 2e-4, "correction": 2e-4, "divergence": 2e-4}
+REL = {"pressure": 2e-4, "correction": 2e-4, "divergence": 2e-4, "liquid": 1e-2}
+# droplets: positions and velocities within 1e-4 (domain units, domain units per second)
+# of the oracle's, ages and masses equal
 
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("precision", [32, 64])
 def test_oracle_reproduces_golden(name, precision):
-    sim = OracleSim(DIMS, CASES[name]["options"](), precision=precision)
+    sim = start(OracleSim(DIMS, CASES[name]["options"](), precision=precision), CASES[name])
     sim.step(CASES[name]["steps"], DT)
     for f in FIELDS:
         assert np.array_equal(sim.read(f), GOLD[f"{name}/fp{precision}/{f}"]), (name, precision, f)
+    assert np.array_equal(sim.read_particles(), GOLD[f"{name}/fp{precision}/particles"]), (name, precision)
     assert sim.state == META["cases"][f"{name}/fp{precision}"]["state"]
     sim.close()
 
@@ -47,10 +50,14 @@ def test_oracle_golden_uniforms_and_mask():
 @pytest.mark.parametrize("name", list(CASES))
 def test_cuda_path_matches_golden(name):
     g = FireXSim(DIMS, CASES[name]["options"]())
-    assert np.array_equal(g.uniforms(DT), GOLD["uniforms_dt_1_60"])  # every case runs the default parameters
     if name == "spheres_warm_f32":
+        assert np.array_equal(g.uniforms(DT), GOLD["uniforms_dt_1_60"])
         assert np.array_equal(g.read("emitter_mask"), GOLD["emitter_mask"])
+    start(g, CASES[name])
     g.step(CASES[name]["steps"], DT)
+    p, q = g.read_particles(), GOLD[f"{name}/fp32/particles"]
+    assert np.array_equal(p[:, 0, 3], q[:, 0, 3]) and np.array_equal(p[:, 1, 3], q[:, 1, 3]), name
+    assert max_abs(p[:, :, :3], q[:, :, :3]) <= 1e-4, (name, max_abs(p[:, :, :3], q[:, :, :3]))
     for f in FIELDS:
         ref = GOLD[f"{name}/fp32/{f}"]
         got = g.read(f)
