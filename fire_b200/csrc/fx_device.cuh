@@ -188,7 +188,7 @@ enum FxShape {
     FX_SHAPE_ZM = 3,
     FX_SHAPE_TAB = 4,
     FX_SHAPE_RES = 5,  // one CTA per box of the resident Jacobi (fx_jacobi_res.cuh)
-    FX_SHAPE_PART = 6, // FX_SPH_THREADS droplets per brick (members whose water runs)
+    FX_SHAPE_PART = 6, // FX_SPH_DROPLETS droplets per brick (members whose water runs)
     FX_NSHAPES = 7
 };
 
@@ -206,7 +206,8 @@ struct FxResBox {
 #define FX_CELL_BY 4
 #define FX_CELL_BZ 2
 #define FX_ROW4_THREADS 256
-#define FX_SPH_THREADS 128  // droplets per brick of the particle passes
+#define FX_SPH_THREADS 256                    // threads of the droplet passes: one warp per droplet
+#define FX_SPH_DROPLETS (FX_SPH_THREADS / 32)  // droplets per brick
 
 struct FxBatchDev {
     int nsims;

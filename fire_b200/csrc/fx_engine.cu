@@ -172,8 +172,8 @@ void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, in
     }
 }
 
-// Launches of the droplet pass (clear, density, integrate, deposit) when a member sprays.
-int sph_launches(const StepPlan& pl) { return pl.bricks[FX_SHAPE_PART] > 0 ? 4 : 0; }
+// Launches of the droplet pass (liquid clear + density, integrate + deposit) when a member sprays.
+int sph_launches(const StepPlan& pl) { return pl.bricks[FX_SHAPE_PART] > 0 ? 2 : 0; }
 
 void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     fx_launch_step_begin(st, B);
@@ -618,7 +618,7 @@ struct firex_batch {
             h->start[FX_SHAPE_TAB][i] = acc[FX_SHAPE_TAB];
             h->start[FX_SHAPE_RES][i] = acc[FX_SHAPE_RES];
             h->start[FX_SHAPE_PART][i] = acc[FX_SHAPE_PART];
-            acc[FX_SHAPE_PART] += s->h.water ? (s->h.np + FX_SPH_THREADS - 1) / FX_SPH_THREADS : 0;
+            acc[FX_SHAPE_PART] += s->h.water ? (s->h.np + FX_SPH_DROPLETS - 1) / FX_SPH_DROPLETS : 0;
             if (resOk) {
                 h->res[i] = boxes[i];
                 acc[FX_SHAPE_RES] += boxes[i].nby * boxes[i].nbz;

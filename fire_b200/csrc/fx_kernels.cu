@@ -424,39 +424,39 @@ __global__ void fxk_emitter_mask(const FxSimDev* __restrict__ S, uint8_t* __rest
 // ---- SPH droplets and liquid deposition (fx_sph.cuh), before simulate --------------------
 // Members whose water runs: clear the liquid field, then density, integration (droplets
 // part[pti] -> part[pti ^ 1]) and deposition; step_end flips pti.
-__global__ void __launch_bounds__(256) fxk_sph_clear(const FxBatchDev* __restrict__ B) {
-    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+// ---- droplets (FIREX_PARTICLE_WGSL, shaders.ts:514-825) -----------------------------------
+// Two launches per step: the liquid clear of every spraying member with the droplet
+// densities, then integration with each droplet's deposit (a droplet deposits only its own
+// old and new state, so it needs no other droplet's result).
+__global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_density(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {  // encoder.clearBuffer(liquid)
         if (!S.water) return;
+        static_assert(FX_SPH_THREADS == FX_ROW4_THREADS, "one ROW4 brick per block");
         const long long i = (long long)b * (FX_ROW4_THREADS * 4) + 4 * threadIdx.x;
         const long long n = (long long)S.X * S.Y * S.Z;
         if (i < n) *reinterpret_cast<uint4*>(S.liquid + i) = make_uint4(0u, 0u, 0u, 0u);  // n % 4 == 0
     });
-}
-__global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_density(const FxBatchDev* __restrict__ B) {
     fx_for_bricks<FX_SHAPE_PART>(B, [&](const FxSimDev& S, int b) {
-        const int i = b * FX_SPH_THREADS + threadIdx.x;
-        if (i >= S.np) return;
+        const int i = b * FX_SPH_DROPLETS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+        if (i >= S.np) return;  // warp-uniform
         const fxsph::Ctx c{S.prm.u, S.X, S.Y, S.Z};
-        S.pdens[i] = fxsph::density(c, S.np, S.part[S.pti], i);
+        const float4 d = fxsph::density_warp(c, S.np, S.part[S.pti], i, lane);
+        if (lane == 0) S.pdens[i] = d;
     });
 }
 __global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_integrate(const FxBatchDev* __restrict__ B) {
     fx_for_bricks<FX_SHAPE_PART>(B, [&](const FxSimDev& S, int b) {
-        const int i = b * FX_SPH_THREADS + threadIdx.x;
-        if (i >= S.np) return;
+        const int i = b * FX_SPH_DROPLETS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+        if (i >= S.np) return;  // warp-uniform
         const fxsph::Ctx c{S.prm.u, S.X, S.Y, S.Z};
+        const float4* pin = S.part[S.pti];
         float4 oa, om;
-        fxsph::integrate(c, S.np, S.part[S.pti], S.pdens, reinterpret_cast<const float4*>(S.flow[S.fi]), i, oa, om);
-        S.part[S.pti ^ 1][2 * i] = oa;
-        S.part[S.pti ^ 1][2 * i + 1] = om;
-    });
-}
-__global__ void __launch_bounds__(FX_SPH_THREADS) fxk_sph_deposit(const FxBatchDev* __restrict__ B) {
-    fx_for_bricks<FX_SHAPE_PART>(B, [&](const FxSimDev& S, int b) {
-        const int i = b * FX_SPH_THREADS + threadIdx.x;
-        if (i >= S.np) return;
-        const fxsph::Ctx c{S.prm.u, S.X, S.Y, S.Z};
-        fxsph::deposit(c, S.part[S.pti], S.part[S.pti ^ 1], S.liquid, i);
+        fxsph::integrate_warp(c, S.np, pin, S.pdens, reinterpret_cast<const float4*>(S.flow[S.fi]), i, lane, oa, om);
+        if (lane == 0) {
+            S.part[S.pti ^ 1][2 * i] = oa;
+            S.part[S.pti ^ 1][2 * i + 1] = om;
+        }
+        fxsph::deposit_warp(c, __ldg(pin + 2 * i), __ldg(pin + 2 * i + 1), oa, om, S.liquid, lane);
     });
 }
 
@@ -814,11 +814,9 @@ void fx_launch_emitter_mask(cudaStream_t s, const FxSimDev* S, uint8_t* mask) {
 }
 
 void fx_launch_sph(cudaStream_t s, const FxBatchDev* B, int rowBricks, int partBricks) {
-    static int g = persistent_grid((const void*)fxk_sph_clear, 256, 1 << 30);
-    fxk_sph_clear<<<row4_grid(g, rowBricks), 256, 0, s>>>(B);
-    fxk_sph_density<<<partBricks, FX_SPH_THREADS, 0, s>>>(B);
+    static int g = persistent_grid((const void*)fxk_sph_density, FX_SPH_THREADS, 1 << 30);
+    fxk_sph_density<<<std::max(partBricks, row4_grid(g, rowBricks)), FX_SPH_THREADS, 0, s>>>(B);
     fxk_sph_integrate<<<partBricks, FX_SPH_THREADS, 0, s>>>(B);
-    fxk_sph_deposit<<<partBricks, FX_SPH_THREADS, 0, s>>>(B);
 }
 
 void fx_launch_pack_sim(cudaStream_t s, const FxSimDev* S) { fxk_pack_sim<<<num_sms() * 8, 256, 0, s>>>(S); }

@@ -74,22 +74,38 @@ FXD int cellIndex(const Ctx& c, int x, int y, int z) {
     return x + c.X * (y + c.Y * z);
 }
 
+// One warp per droplet. Lane l tests neighbour base + l of each run of 32; the warp then
+// adds the terms of the neighbours in range in index order (ballot, then one shuffle per
+// term), so every sum has the reference's order and rounding while the distance tests run
+// 32 wide. Every lane ends with the same sums.
+#define FX_FULL_MASK 0xffffffffu
+
 // computeParticleDensity for droplet i (shaders.ts:602-638); p: 2 float4 per droplet
-FXD float4 density(const Ctx& c, int n, const float4* __restrict__ p, int i) {
-    const float4 pa = p[2 * i], vm = p[2 * i + 1];
+FXD float4 density_warp(const Ctx& c, int n, const float4* __restrict__ p, int i, int lane) {
+    const float4 pa = __ldg(p + 2 * i), vm = __ldg(p + 2 * i + 1);
     if (vm.w <= 0.0001f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float3 ext = c.ext();
     const float r = c.spray() ? 0.060f : 0.038f;
     float de = 0.0f, near = 0.0f;
-    for (int j = 0; j < n; ++j) {
-        if (j == i) continue;
-        const float4 qa = p[2 * j], qm = p[2 * j + 1];
-        if (qm.w <= 0.0001f) continue;
-        const float dist = len(mul(sub(make_float3(pa.x, pa.y, pa.z), make_float3(qa.x, qa.y, qa.z)), ext));
-        if (dist > 0.00001f && dist < r) {
-            const float w = 1.0f - dist / r;
-            de += w * w;
-            near += w * w * w;
+    for (int base = 0; base < n; base += 32) {
+        const int j = base + lane;
+        float w = 0.0f;
+        bool hit = false;
+        if (j < n && j != i) {
+            const float4 qa = __ldg(p + 2 * j), qm = __ldg(p + 2 * j + 1);
+            if (!(qm.w <= 0.0001f)) {
+                const float dist = len(mul(sub(make_float3(pa.x, pa.y, pa.z), make_float3(qa.x, qa.y, qa.z)), ext));
+                if (dist > 0.00001f && dist < r) {
+                    w = 1.0f - dist / r;
+                    hit = true;
+                }
+            }
+        }
+        const float w2 = w * w, w3 = w * w * w;
+        for (unsigned m = __ballot_sync(FX_FULL_MASK, hit); m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            de += __shfl_sync(FX_FULL_MASK, w2, src);
+            near += __shfl_sync(FX_FULL_MASK, w3, src);
         }
     }
     const float rest = 2.7f + c.u[12] * 0.9f;
@@ -97,9 +113,9 @@ FXD float4 density(const Ctx& c, int n, const float4* __restrict__ p, int i) {
 }
 
 // integrateParticles for droplet i (shaders.ts:640-736); flow: the canonical flow field
-FXD void integrate(const Ctx& c, int n, const float4* __restrict__ p, const float4* __restrict__ dens,
-                   const float4* __restrict__ flow, int i, float4& oa, float4& om) {
-    const float4 pa = p[2 * i], vm = p[2 * i + 1];
+FXD void integrate_warp(const Ctx& c, int n, const float4* __restrict__ p, const float4* __restrict__ dens,
+                        const float4* __restrict__ flow, int i, int lane, float4& oa, float4& om) {
+    const float4 pa = __ldg(p + 2 * i), vm = __ldg(p + 2 * i + 1);
     const float dt = c.u[4];
     if (dt <= 0.0f) {
         oa = pa;
@@ -135,29 +151,44 @@ FXD void integrate(const Ctx& c, int n, const float4* __restrict__ p, const floa
     const float r = c.spray() ? 0.060f : 0.038f;
     const float3 pos = make_float3(pa.x, pa.y, pa.z);
     float3 vel = make_float3(vm.x, vm.y, vm.z);
-    const float4 pd = dens[i];
+    const float4 pd = __ldg(dens + i);
     float3 pacc = make_float3(0.0f, 0.0f, 0.0f), vacc = pacc;
-    for (int j = 0; j < n; ++j) {
-        if (j == i) continue;
-        const float4 qa = p[2 * j], qm = p[2 * j + 1];
-        if (qm.w <= 0.0001f) continue;
-        const float3 sep = mul(sub(pos, make_float3(qa.x, qa.y, qa.z)), ext);
-        const float dist = len(sep);
-        if (dist > 0.00001f && dist < r) {
-            const float w = 1.0f - dist / r;
-            const float3 dir = divs(sep, dist);
-            const float4 nd = dens[j];
-            const float pr = (pd.z + nd.z) * w;
-            const float npr = (pd.w + nd.w) * w * w;
-            pacc = add(pacc, muls(dir, pr + npr));
-            vacc = add(vacc, muls(sub(make_float3(qm.x, qm.y, qm.z), vel), w * 0.018f));
+    for (int base = 0; base < n; base += 32) {
+        const int j = base + lane;
+        float3 tp = make_float3(0.0f, 0.0f, 0.0f), tv = tp;
+        bool hit = false;
+        if (j < n && j != i) {
+            const float4 qa = __ldg(p + 2 * j), qm = __ldg(p + 2 * j + 1);
+            if (!(qm.w <= 0.0001f)) {
+                const float3 sep = mul(sub(pos, make_float3(qa.x, qa.y, qa.z)), ext);
+                const float dist = len(sep);
+                if (dist > 0.00001f && dist < r) {
+                    const float w = 1.0f - dist / r;
+                    const float3 dir = divs(sep, dist);
+                    const float4 nd = __ldg(dens + j);
+                    const float pr = (pd.z + nd.z) * w;
+                    const float npr = (pd.w + nd.w) * w * w;
+                    tp = muls(dir, pr + npr);
+                    tv = muls(sub(make_float3(qm.x, qm.y, qm.z), vel), w * 0.018f);
+                    hit = true;
+                }
+            }
+        }
+        for (unsigned m = __ballot_sync(FX_FULL_MASK, hit); m; m &= m - 1) {
+            const int src = __ffs(m) - 1;
+            pacc.x += __shfl_sync(FX_FULL_MASK, tp.x, src);
+            pacc.y += __shfl_sync(FX_FULL_MASK, tp.y, src);
+            pacc.z += __shfl_sync(FX_FULL_MASK, tp.z, src);
+            vacc.x += __shfl_sync(FX_FULL_MASK, tv.x, src);
+            vacc.y += __shfl_sync(FX_FULL_MASK, tv.y, src);
+            vacc.z += __shfl_sync(FX_FULL_MASK, tv.z, src);
         }
     }
     // sampleFlow: nearest cell of the canonical flow
     const int cx = (int)(fx_clamp(pos.x, 0.0f, 0.99999f) * c.u[0]);
     const int cy = (int)(fx_clamp(pos.y, 0.0f, 0.99999f) * c.u[1]);
     const int cz = (int)(fx_clamp(pos.z, 0.0f, 0.99999f) * c.u[2]);
-    const float4 g = flow[cellIndex(c, cx, cy, cz)];
+    const float4 g = __ldg(flow + cellIndex(c, cx, cy, cz));
     const float heat = fx_smoothstep(380.0f, 1500.0f, g.w);
     float3 acc = make_float3(0.0f, -0.58f, 0.0f);
     acc = add(acc, muls(sub(make_float3(g.x, g.y, g.z), vel), 0.30f + heat * 0.18f));
@@ -184,61 +215,51 @@ FXD void integrate(const Ctx& c, int n, const float4* __restrict__ p, const floa
     om = make_float4(fx_clamp(vel.x, -2.0f, 2.0f), fx_clamp(vel.y, -2.0f, 2.0f), fx_clamp(vel.z, -2.0f, 2.0f), mass);
 }
 
-// depositParticles (shaders.ts:738-824)
+// depositParticles (shaders.ts:738-824): integer sums, exact in any order, so the corners
+// of a footprint go to separate lanes (8 trilinear corners for the jet, 27 cells for the
+// spray, whose normalising total is added in the reference's z, y, x order by shuffles).
 FXD void corner(const Ctx& c, uint32_t* liq, int x, int y, int z, float weight, float mass) {
     const uint32_t fixed = (uint32_t)fx_clamp(weight * mass * 4096.0f, 0.0f, 65535.0f);
     atomicAdd(liq + cellIndex(c, x, y, z), fixed);
 }
-FXD void depositAt(const Ctx& c, uint32_t* liq, float3 position, float mass) {
+FXD void depositAt_warp(const Ctx& c, uint32_t* liq, float3 position, float mass, int lane) {
     const float3 vp = sub(mul(position, make_float3(c.u[0], c.u[1], c.u[2])), make_float3(0.5f, 0.5f, 0.5f));
     if (!c.spray()) {
-        const int bx = (int)floorf(vp.x), by = (int)floorf(vp.y), bz = (int)floorf(vp.z);
+        if (lane >= 8) return;
+        const int dx = lane & 1, dy = (lane >> 1) & 1, dz = lane >> 2;
         const float3 f = make_float3(fract(vp.x), fract(vp.y), fract(vp.z));
         const float3 iv = make_float3(1.0f - f.x, 1.0f - f.y, 1.0f - f.z);
-        const float m = mass * 0.20f;
-        corner(c, liq, bx, by, bz, iv.x * iv.y * iv.z, m);
-        corner(c, liq, bx + 1, by, bz, f.x * iv.y * iv.z, m);
-        corner(c, liq, bx, by + 1, bz, iv.x * f.y * iv.z, m);
-        corner(c, liq, bx + 1, by + 1, bz, f.x * f.y * iv.z, m);
-        corner(c, liq, bx, by, bz + 1, iv.x * iv.y * f.z, m);
-        corner(c, liq, bx + 1, by, bz + 1, f.x * iv.y * f.z, m);
-        corner(c, liq, bx, by + 1, bz + 1, iv.x * f.y * f.z, m);
-        corner(c, liq, bx + 1, by + 1, bz + 1, f.x * f.y * f.z, m);
+        const float weight = (dx ? f.x : iv.x) * (dy ? f.y : iv.y) * (dz ? f.z : iv.z);
+        corner(c, liq, (int)floorf(vp.x) + dx, (int)floorf(vp.y) + dy, (int)floorf(vp.z) + dz, weight, mass * 0.20f);
         return;
     }
     const int cx = (int)rintf(vp.x), cy = (int)rintf(vp.y), cz = (int)rintf(vp.z);
+    const int ox = lane % 3 - 1, oy = (lane / 3) % 3 - 1, oz = lane / 9 - 1;  // lane = 9 (oz+1) + 3 (oy+1) + ox+1
+    float kk = 0.0f;
+    if (lane < 27) {
+        const float d = len(sub(vp, make_float3((float)(cx + ox), (float)(cy + oy), (float)(cz + oz))));
+        const float k = fx_max(0.0f, 1.0f - d * 0.52f);
+        kk = k * k;
+    }
     float total = 0.0f;
-    for (int oz = -1; oz <= 1; ++oz)
-        for (int oy = -1; oy <= 1; ++oy)
-            for (int ox = -1; ox <= 1; ++ox) {
-                const float d = len(sub(vp, make_float3((float)(cx + ox), (float)(cy + oy), (float)(cz + oz))));
-                const float k = fx_max(0.0f, 1.0f - d * 0.52f);
-                total += k * k;
-            }
-    for (int oz = -1; oz <= 1; ++oz)
-        for (int oy = -1; oy <= 1; ++oy)
-            for (int ox = -1; ox <= 1; ++ox) {
-                const float d = len(sub(vp, make_float3((float)(cx + ox), (float)(cy + oy), (float)(cz + oz))));
-                const float k = fx_max(0.0f, 1.0f - d * 0.52f);
-                corner(c, liq, cx + ox, cy + oy, cz + oz, k * k / fx_max(total, 0.0001f), mass);
-            }
+    for (int l = 0; l < 27; ++l) total += __shfl_sync(FX_FULL_MASK, kk, l);
+    if (lane < 27) corner(c, liq, cx + ox, cy + oy, cz + oz, kk / fx_max(total, 0.0001f), mass);
 }
-FXD void deposit(const Ctx& c, const float4* __restrict__ pin, const float4* __restrict__ pout, uint32_t* liq, int i) {
-    const float4 oa = pout[2 * i], om = pout[2 * i + 1];
+// pa, pm: the droplet before the step; oa, om: after it
+FXD void deposit_warp(const Ctx& c, float4 pa, float4 pm, float4 oa, float4 om, uint32_t* liq, int lane) {
     const float3 pos = make_float3(oa.x, oa.y, oa.z);
     const float mass = om.w;
     if (mass <= 0.0001f || pos.x < 0.0f || pos.y < 0.0f || pos.z < 0.0f || pos.x >= 1.0f || pos.y >= 1.0f || pos.z >= 1.0f)
         return;
-    const float4 pa = pin[2 * i], pm = pin[2 * i + 1];
     const float3 disp = sub(pos, make_float3(pa.x, pa.y, pa.z));
     const bool sweep = pm.w > 0.0001f && oa.w >= pa.w && len(mul(disp, c.ext())) < 0.20f;
     if (!sweep) {
-        depositAt(c, liq, pos, mass);
+        depositAt_warp(c, liq, pos, mass, lane);
         return;
     }
     for (unsigned k = 0; k < 3u; ++k) {
         const float fr = (float)k / 2.0f;
-        depositAt(c, liq, add(make_float3(pa.x, pa.y, pa.z), muls(disp, fr)), mass / 3.0f);
+        depositAt_warp(c, liq, add(make_float3(pa.x, pa.y, pa.z), muls(disp, fr)), mass / 3.0f, lane);
     }
 }
 
