@@ -121,6 +121,23 @@ class Options(C.Structure):
     ]
 
 
+class DeviceLimits(C.Structure):
+    _fields_ = [("max_texture_dimension_3d", C.c_uint64), ("max_storage_buffer_binding_size", C.c_uint64),
+                ("max_buffer_size", C.c_uint64)]
+
+
+class PreflightResult(C.Structure):
+    _fields_ = [("issues", C.c_uint32), ("issue_count", C.c_uint32), ("cell_count", C.c_uint64),
+                ("grid_bytes", C.c_uint64), ("particle_bytes", C.c_uint64), ("fixed_bytes", C.c_uint64),
+                ("total_bytes", C.c_uint64), ("largest_storage_buffer_bytes", C.c_uint64),
+                ("planned_device_bytes", C.c_uint64), ("message", C.c_char * 1024)]
+
+
+# preflight issue bits and the reference's codes (gridConfiguration.ts:297-350)
+ISSUE_CODES = {0x01: "invalid-dimension", 0x02: "unaligned-dimension", 0x04: "texture-dimension-limit",
+               0x08: "storage-binding-limit", 0x10: "buffer-size-limit", 0x20: "memory-budget"}
+
+
 class Diagnostics(C.Structure):
     _fields_ = [
         ("fast_division", C.c_int32),
@@ -175,6 +192,7 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_get_info": (C.c_int, [vp, DIMS, C.POINTER(Options)]),
         "firex_device_bytes": (C.c_int, [vp, C.POINTER(C.c_uint64)]),
         "firex_reference_memory_estimate": (C.c_uint64, [DIMS, C.c_int64]),
+        "firex_preflight": (C.c_int, [DIMS, C.POINTER(Options), C.POINTER(DeviceLimits), C.POINTER(PreflightResult)]),
         "firex_stream": (vp, [vp]),
         "firex_set_profiling": (C.c_int, [vp, C.c_int32]),
         "firex_pass_times": (C.c_int, [vp, C.POINTER(C.c_double), C.POINTER(C.c_int64)]),
@@ -207,7 +225,7 @@ HEADER_SYMBOLS = [
     "firex_set_render_packing", "firex_render_volumes", "firex_read_particles", "firex_write_particles",
     "firex_divergence_norm_noalloc", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
-    "firex_reference_memory_estimate", "firex_stream", "firex_set_profiling", "firex_pass_times",
+    "firex_reference_memory_estimate", "firex_preflight", "firex_stream", "firex_set_profiling", "firex_pass_times",
     "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_batch_create", "firex_batch_destroy",
     "firex_batch_add", "firex_batch_remove", "firex_batch_size", "firex_batch_step", "firex_batch_sync",
     "firex_batch_last_error", "firex_batch_stream",

@@ -1051,6 +1051,51 @@ uint64_t firex_reference_memory_estimate(const int32_t dims[3], int64_t particle
     return cells * per + (uint64_t)std::max<int64_t>(particle_count, 0) * 80 + 64ull * 64 * 64 * 4;
 }
 
+int firex_preflight(const int32_t dims[3], const firex_options* opt, const firex_device_limits* limits,
+                    firex_preflight_result* out) {
+    if (!dims || !opt || !out) return FIREX_ERR_BAD_ARG;
+    std::memset(out, 0, sizeof(*out));
+    firex_device_limits own = {2048, ((1ull << 31) - 1) * 16, ((1ull << 31) - 1) * 16};
+    const firex_device_limits& L = limits ? *limits : own;
+    const int64_t particles = std::max<int32_t>(opt->particle_count, 0);
+    out->cell_count = (uint64_t)std::max(dims[0], 0) * (uint64_t)std::max(dims[1], 0) * (uint64_t)std::max(dims[2], 0);
+    out->grid_bytes = out->cell_count * (out->cell_count >= (uint64_t)FIREX_HEAVY_GRID_CELL_THRESHOLD ? 108 : 116);
+    out->particle_bytes = (uint64_t)particles * 80;
+    out->fixed_bytes = 64ull * 64 * 64 * 4;
+    out->total_bytes = out->grid_bytes + out->particle_bytes + out->fixed_bytes;
+    out->largest_storage_buffer_bytes = out->cell_count * 16;
+    std::string msg;
+    auto issue = [&](uint32_t bit, const char* code, const std::string& text) {
+        out->issues |= bit;
+        out->issue_count += 1;
+        msg += (msg.empty() ? "" : "; ") + std::string(code) + ": " + text;
+    };
+    const char* label[3] = {"X", "Y", "Z"};
+    for (int i = 0; i < 3; ++i) {
+        if (dims[i] <= 0)
+            issue(FIREX_ISSUE_INVALID_DIMENSION, "invalid-dimension", std::string(label[i]) + " must be a positive integer.");
+        else if (dims[i] % 4 != 0)
+            issue(FIREX_ISSUE_UNALIGNED_DIMENSION, "unaligned-dimension", std::string(label[i]) + " must be a multiple of 4.");
+        if (dims[i] > 0 && (uint64_t)dims[i] > L.max_texture_dimension_3d)
+            issue(FIREX_ISSUE_TEXTURE_DIMENSION_LIMIT, "texture-dimension-limit",
+                  std::string(label[i]) + "=" + std::to_string(dims[i]) + " exceeds this device's 3D-texture limit of " +
+                      std::to_string(L.max_texture_dimension_3d) + ".");
+    }
+    if (out->largest_storage_buffer_bytes > L.max_storage_buffer_binding_size)
+        issue(FIREX_ISSUE_STORAGE_BINDING_LIMIT, "storage-binding-limit",
+              "A Fire-X vector field exceeds the storage-binding limit.");
+    if (out->largest_storage_buffer_bytes > L.max_buffer_size)
+        issue(FIREX_ISSUE_BUFFER_SIZE_LIMIT, "buffer-size-limit", "A Fire-X vector field exceeds the buffer limit.");
+    if (opt->memory_budget_bytes && out->total_bytes > opt->memory_budget_bytes)
+        issue(FIREX_ISSUE_MEMORY_BUDGET, "memory-budget",
+              "Estimated persistent Fire-X resources require " + std::to_string(out->total_bytes) +
+                  " bytes, above the configured " + std::to_string(opt->memory_budget_bytes) + " budget.");
+    if (!(out->issues & (FIREX_ISSUE_INVALID_DIMENSION | FIREX_ISSUE_UNALIGNED_DIMENSION)))
+        out->planned_device_bytes = firex_planned_device_bytes(dims, opt);
+    std::snprintf(out->message, sizeof(out->message), "%s", msg.c_str());
+    return FIREX_OK;
+}
+
 uint64_t firex_planned_device_bytes(const int32_t dims[3], const firex_options* opt) {
     if (!dims || !opt) return 0;
     const long long N = (long long)std::max(dims[0], 0) * std::max(dims[1], 0) * std::max(dims[2], 0);
@@ -1067,11 +1112,16 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         g_create_error = "dims and options are required";
         return FIREX_ERR_BAD_ARG;
     }
-    for (int i = 0; i < 3; ++i)
-        if (dims[i] < 4 || dims[i] % 4 != 0 || dims[i] > 2048) {
-            g_create_error = "grid axes must be positive multiples of 4 and at most 2048";
+    {
+        firex_preflight_result pre;
+        firex_options o = *opt;
+        o.memory_budget_bytes = 0;  // the budget is checked below against the planned residency
+        firex_preflight(dims, &o, nullptr, &pre);
+        if (pre.issues) {
+            g_create_error = std::string("grid refused: ") + pre.message;
             return FIREX_ERR_BAD_ARG;
         }
+    }
     if (opt->pressure_iterations < 0 || opt->correction_iterations < 0 || opt->pressure_iterations > 100000 ||
         opt->correction_iterations > 100000 || opt->num_spheres < 0 || opt->num_spheres > FIREX_MAX_SPHERES ||
         (opt->emitter_mode != FIREX_EMITTER_BURNER && opt->emitter_mode != FIREX_EMITTER_SPHERES) ||
@@ -1081,17 +1131,13 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         g_create_error = "invalid options";
         return FIREX_ERR_BAD_ARG;
     }
-    const long long N = (long long)dims[0] * dims[1] * dims[2];
-    if (N >= (1LL << 31)) {
-        g_create_error = "grid has 2^31 cells or more";
-        return FIREX_ERR_BAD_ARG;
-    }
+    const long long N = (long long)dims[0] * dims[1] * dims[2];  // below 2^31: the preflight's buffer limits
     int mode = opt->pressure_mode;
     if (mode == FIREX_PRESSURE_AUTO) mode = N >= FIREX_HEAVY_GRID_CELL_THRESHOLD ? FIREX_PRESSURE_F16 : FIREX_PRESSURE_WARM_F32;
     const int storage = opt->precision == FIREX_PRECISION_MIXED ? FX_STORAGE_MIXED : FX_STORAGE_F32;
     const size_t need = firex_sim::planned_bytes(dims[0], dims[1], dims[2], storage, mode, opt->particle_count);
     if (opt->memory_budget_bytes && need > opt->memory_budget_bytes) {
-        g_create_error = "grid needs " + std::to_string(need) + " device bytes, above the " +
+        g_create_error = "memory-budget: grid needs " + std::to_string(need) + " device bytes, above the " +
                          std::to_string(opt->memory_budget_bytes) + "-byte budget";
         return FIREX_ERR_BUDGET;
     }

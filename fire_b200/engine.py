@@ -126,6 +126,7 @@ class FireXEngine:
         self.initialized = False
         self.disposed = False
         self.paused = False
+        self.renderPacking = False
 
     # -- configuration ------------------------------------------------------------------------
     def activeConfiguration(self) -> QualityConfiguration:
@@ -178,10 +179,13 @@ class FireXEngine:
             raise FireXError(A.ERR_BUDGET, " ".join(issues))
         cfg = self.activeConfiguration()
         opts = make_options(pressure_iterations=cfg.pressureIterations, correction_iterations=cfg.correctionIterations,
-                            cinematic=self.usesCinematicPresentation(), **self._extra_options)
+                            cinematic=self.usesCinematicPresentation(), particle_count=cfg.particleCount,
+                            **self._extra_options)
         replacement = self._factory(tuple(dimensions), opts)
         for name, value in self._params.items():
             replacement.set_parameter(name, value)
+        if self.renderPacking and hasattr(replacement, "set_render_packing"):
+            replacement.set_render_packing(True)
         replacement.reset()  # installResourceSet -> initializeFields with the current parameters
         previous, self._sim = self._sim, replacement
         self.clock.reset()
@@ -302,24 +306,53 @@ class FireXEngine:
         return (time.perf_counter() - start) * 1e3
 
     def renderOfflineFrame(self, deltaSeconds: float, present: bool = True, signal=None) -> None:
-        """Offline path (FireXEngine.ts:651-697): exact equal sub-steps, then wait."""
+        """Offline path (FireXEngine.ts:651-697): exact equal sub-steps, then wait. With
+        `present`, the last sub-step also packs the render volumes (the headless stand-in for
+        the presentation pass and its beauty volumes, qualityShaders.ts:77-87); a CPU
+        simulation without device volumes packs on read instead."""
         if not math.isfinite(deltaSeconds) or deltaSeconds < 0:
             raise ValueError("Offline frame delta must be finite and non-negative.")
         if self._sim is None:
             raise RuntimeError("engine is not initialised")
         self.clock.reset()
-        for dt in splitOfflineSimulationDelta(deltaSeconds, self.activeConfiguration().timeStep):
+        steps = splitOfflineSimulationDelta(deltaSeconds, self.activeConfiguration().timeStep)
+        packs = present and hasattr(self._sim, "set_render_packing")
+        for i, dt in enumerate(steps):
             if signal is not None and getattr(signal, "aborted", False):
                 raise InterruptedError("Offline render canceled.")
-            self._sim.step(1, dt)
+            last = packs and i == len(steps) - 1 and not self.renderPacking
+            if last:
+                self._sim.set_render_packing(True)
+            try:
+                self._sim.step(1, dt)
+            finally:
+                if last:
+                    self._sim.set_render_packing(False)
         if hasattr(self._sim, "sync"):
             self._sim.sync()
+
+    def setRenderPacking(self, on: bool) -> None:
+        """Pack the render volumes at the end of every step (a renderer on the same device
+        reads them through renderVolumes())."""
+        self.renderPacking = bool(on)
+        if self._sim is not None and hasattr(self._sim, "set_render_packing"):
+            self._sim.set_render_packing(self.renderPacking)
+
+    def renderVolumes(self) -> list:
+        """Device addresses of the flow, chemistry and media volumes (0 before first use)."""
+        return self._sim.render_volumes() if hasattr(self._sim, "render_volumes") else [0, 0, 0]
 
     # -- readback (added for the drop-in) -------------------------------------------------------
     def readField(self, name: str) -> np.ndarray:
         if self._sim is None:
             raise RuntimeError("engine is not initialised")
         return self._sim.read(name)
+
+    def readParticles(self) -> np.ndarray:
+        """Droplets as (particleCount, 2, 4) float32: (x, y, z, age), (vx, vy, vz, mass)."""
+        if self._sim is None:
+            raise RuntimeError("engine is not initialised")
+        return self._sim.read_particles()
 
     def divergenceNorm(self) -> tuple:
         return self._sim.divergence_norm()

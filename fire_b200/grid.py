@@ -146,3 +146,27 @@ def device_bytes_per_cell(precision: int = A.PRECISION_F32, pressure_mode: int =
     pbytes = 2 if pressure_mode == A.PRESSURE_F16 else 4
     npress = 2 if pressure_mode == A.PRESSURE_COLD_F32 else 4
     return 16 * 2 + species * 2 + pbytes * npress + 4 * 4
+
+
+def library_preflight(dimensions, options=None, limits: dict | None = None) -> PreflightResult:
+    """firex_preflight through the C ABI: the same checks and codes, evaluated natively
+    (limits None: the library's own). options carry particle_count and
+    memory_budget_bytes (0 = no budget)."""
+    import ctypes as C
+
+    from .sim import load_library, make_options
+
+    lib = load_library()
+    opts = options if options is not None else make_options()
+    lim = None
+    if limits is not None:
+        lim = A.DeviceLimits(int(limits["maxTextureDimension3D"]), int(limits["maxStorageBufferBindingSize"]),
+                             int(limits["maxBufferSize"]))
+    r = A.PreflightResult()
+    rc = lib.firex_preflight(A.DIMS(*dimensions), C.byref(opts), C.byref(lim) if lim is not None else None, C.byref(r))
+    if rc != A.OK:
+        raise ValueError("firex_preflight refused its arguments")
+    est = MemoryEstimate(r.cell_count, r.grid_bytes, r.particle_bytes, r.fixed_bytes, r.total_bytes,
+                         r.largest_storage_buffer_bytes)
+    issues = [PreflightIssue(*part.split(": ", 1)) for part in r.message.decode().split("; ") if part]
+    return PreflightResult(r.issues == 0, tuple(dimensions), est, issues)

@@ -246,6 +246,39 @@ int firex_device_bytes(const firex_sim* sim, uint64_t* bytes);
  * or above, + 80 B/particle + the 64^3 RGBA8 detail texture. */
 uint64_t firex_reference_memory_estimate(const int32_t dims[3], int64_t particle_count);
 
+/* Grid preflight (preflightFireXGrid, gridConfiguration.ts:297-350): the reference's
+ * checks and issue codes, one bit per code, evaluated on the host before any device
+ * memory is touched. The estimate is the reference's model (as above) for
+ * opt->particle_count droplets; the budget check compares it with
+ * opt->memory_budget_bytes (0 = no budget check). limits NULL takes this library's own:
+ * at most 2048 cells per axis and fewer than 2^31 cells (16-byte vector fields up to
+ * (2^31 - 1) * 16 bytes). firex_create refuses a grid with any of the first five issues
+ * (FIREX_ERR_BAD_ARG) and answers the budget with FIREX_ERR_BUDGET against its own
+ * planned residency; its error text names the issue codes. */
+#define FIREX_ISSUE_INVALID_DIMENSION 0x01u       /* "invalid-dimension" */
+#define FIREX_ISSUE_UNALIGNED_DIMENSION 0x02u     /* "unaligned-dimension" */
+#define FIREX_ISSUE_TEXTURE_DIMENSION_LIMIT 0x04u /* "texture-dimension-limit" */
+#define FIREX_ISSUE_STORAGE_BINDING_LIMIT 0x08u   /* "storage-binding-limit" */
+#define FIREX_ISSUE_BUFFER_SIZE_LIMIT 0x10u       /* "buffer-size-limit" */
+#define FIREX_ISSUE_MEMORY_BUDGET 0x20u           /* "memory-budget" */
+
+typedef struct firex_device_limits {
+    uint64_t max_texture_dimension_3d;        /* cells per axis */
+    uint64_t max_storage_buffer_binding_size; /* bytes */
+    uint64_t max_buffer_size;                 /* bytes */
+} firex_device_limits;
+
+typedef struct firex_preflight_result {
+    uint32_t issues;      /* FIREX_ISSUE_* bits; 0 = ok */
+    uint32_t issue_count; /* issues found, one per axis for the per-axis codes */
+    uint64_t cell_count, grid_bytes, particle_bytes, fixed_bytes, total_bytes, largest_storage_buffer_bytes;
+    uint64_t planned_device_bytes; /* this library's residency for the grid (0 if the grid is refused) */
+    char message[1024];            /* "code: message" of each issue in the reference's order, '; '-separated */
+} firex_preflight_result;
+
+int firex_preflight(const int32_t dims[3], const firex_options* opt, const firex_device_limits* limits,
+                    firex_preflight_result* out);
+
 /* CUDA stream the handle runs on (cudaStream_t as void*), for callers that order their
  * own work after a step. */
 void* firex_stream(const firex_sim* sim);

@@ -57,6 +57,48 @@ def test_preflight_issue_codes():
     assert ok.ok and ok.estimate.totalBytes < G.FIREX_DEFAULT_GRID_MEMORY_BUDGET_BYTES
 
 
+@pytest.mark.parametrize("dims,limits,particles,budget", [
+    ((255, 512, 128), {"maxTextureDimension3D": 256, "maxStorageBufferBindingSize": 128 * 1024 * 1024,
+                       "maxBufferSize": 64 * 1024 * 1024}, 0, G.FIREX_DEFAULT_GRID_MEMORY_BUDGET_BYTES),
+    ((128, 192, 128), {"maxTextureDimension3D": 2048, "maxStorageBufferBindingSize": 1 << 30,
+                       "maxBufferSize": 1 << 30}, 2048, G.FIREX_DEFAULT_GRID_MEMORY_BUDGET_BYTES),
+    ((0, -4, 6), {"maxTextureDimension3D": 4, "maxStorageBufferBindingSize": 1 << 40, "maxBufferSize": 1 << 40}, 640, 0),
+    ((508, 508, 508), {"maxTextureDimension3D": 2048, "maxStorageBufferBindingSize": 1 << 31,
+                       "maxBufferSize": 1 << 32}, 4096, 16 * 1024 ** 3),
+    ((1024, 256, 256), {"maxTextureDimension3D": 1024, "maxStorageBufferBindingSize": 1 << 40,
+                        "maxBufferSize": 1 << 40}, 4096, 4 * 1024 ** 3),
+])
+def test_library_preflight_matches_reference_restatement(dims, limits, particles, budget):
+    """firex_preflight gives the reference's issue codes, in its order, and its estimate."""
+    from fire_b200.sim import make_options
+
+    opts = make_options(particle_count=particles)
+    opts.memory_budget_bytes = budget
+    native = G.library_preflight(dims, opts, limits)
+    ref = G.preflightFireXGrid(dims, limits, particleCount=particles, memoryBudgetBytes=budget or None)
+    assert native.ok == ref.ok
+    assert [i.code for i in native.issues] == [i.code for i in ref.issues]
+    assert [i.message for i in native.issues] == [i.message for i in ref.issues]
+    if all(d > 0 for d in dims):
+        assert native.estimate == ref.estimate
+
+
+def test_library_preflight_own_limits_and_create_admission():
+    from fire_b200.sim import make_options
+
+    opts = make_options()
+    assert G.library_preflight((508, 508, 508), opts).ok
+    r = G.library_preflight((2052, 2048, 2048), opts)
+    assert [i.code for i in r.issues] == ["texture-dimension-limit", "storage-binding-limit", "buffer-size-limit"]
+    lib = load_library()
+    h = C.c_void_p()
+    assert lib.firex_create(A.DIMS(2048, 1024, 1024), C.byref(opts), C.byref(h)) == A.ERR_BAD_ARG
+    assert b"storage-binding-limit" in lib.firex_last_error(None)
+    assert lib.firex_create(A.DIMS(64, 0, 64), C.byref(opts), C.byref(h)) == A.ERR_BAD_ARG
+    assert b"invalid-dimension" in lib.firex_last_error(None)
+    assert not h.value
+
+
 def test_dense_cube_axis_limit():
     assert G.maximumFireXDeviceDenseCubeAxis({"maxTextureDimension3D": 2048,
                                               "maxStorageBufferBindingSize": 512 ** 3 * 16,
@@ -127,6 +169,20 @@ def test_engine_offline_frame_advances_time_and_frames():
     e.dispose()
 
 
+def test_engine_droplets_follow_the_tier_and_the_water_switch():
+    e = _engine()
+    e.initialize()
+    assert e.readParticles().shape == (384, 2, 4)  # the low tier's particleCount
+    e.setParameter("waterEnabled", True)
+    e.setParameter("waterFlow", 0.7)
+    e.renderOfflineFrame(1 / 15)
+    assert (e.readParticles()[:, 1, 3] > 0).any() and e.readField("liquid").any()
+    e.setParameter("waterEnabled", False)
+    e.renderOfflineFrame(1 / 30)
+    assert not e.readField("liquid").any()
+    e.dispose()
+
+
 def test_engine_rebuild_is_transactional():
     e = _engine()
     e.initialize()
@@ -181,7 +237,7 @@ def test_create_rejects_bad_arguments_without_a_device():
     o = A.Options()
     lib.firex_default_options(C.byref(o))
     assert lib.firex_create(A.DIMS(63, 96, 64), C.byref(o), C.byref(h)) == A.ERR_BAD_ARG
-    assert b"multiples of 4" in lib.firex_last_error(None)
+    assert b"unaligned-dimension: X must be a multiple of 4." in lib.firex_last_error(None)
     o.num_spheres = 99
     assert lib.firex_create(A.DIMS(64, 96, 64), C.byref(o), C.byref(h)) == A.ERR_BAD_ARG
     lib.firex_default_options(C.byref(o))

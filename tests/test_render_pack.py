@@ -92,3 +92,28 @@ def test_packing_at_step_end_equals_packing_on_read():
     for a, b in zip(at_step, on_read):
         assert np.array_equal(a, b)
     assert g.diagnostics["launches_per_step"] == 11  # the packing pass joins the step
+
+
+@pytest.mark.gpu
+def test_offline_frame_presentation_packs_the_last_step():
+    """renderOfflineFrame(present=True) leaves the render volumes of the final state on the
+    device (the headless presentation); present=False leaves them as they were."""
+    from fire_b200.engine import FireXEngine
+
+    e = FireXEngine(quality="low")
+    e.initialize()
+    e.setParameter("waterEnabled", True)
+    e.setParameter("waterFlow", 0.6)
+    e.renderOfflineFrame(1 / 15, present=True)
+    sim = e.simulation
+    X, Y, Z = sim.dims
+    ptrs = e.renderVolumes()
+    assert all(ptrs)
+    packed = [_device_u16(p, (Z, Y, X, 4)) for p in ptrs]
+    fresh = [sim.read(n) for n in ("render_flow", "render_chemistry", "render_media")]
+    for a, b in zip(packed, fresh):
+        assert np.array_equal(a, b)
+    assert packed[2][..., 2].any()  # the media volume carries the sprayed liquid
+    e.renderOfflineFrame(1 / 30, present=False)
+    assert np.array_equal(_device_u16(ptrs[0], (Z, Y, X, 4)), packed[0])
+    e.dispose()
