@@ -221,7 +221,23 @@ bool res_box(int X, int Y, int Z, int m, int variant, FxResBox* out) {
         if (fx_res_smem_bytes(X, by, bz) > FX_RES_SMEM_MAX) continue;
         const long long G = (long long)by * bz * gx;
         double work;
-        if (variant != 0) {
+        if (variant == 3) {
+            // faces dealt out; interior columns (rows off the y faces x groups) one per
+            // thread, split along z when there are fewer columns than threads
+            if (2LL * (by + bz) * gx > (long long)FX_RES_MAXF * FX_RES_THREADS) continue;
+            // the most interior rows and planes a box can have: a box with a neighbour on
+            // one side only keeps all but one row (plane) off its faces
+            const int nbzHere = (Z + bz - 1) / bz;
+            const long long rowsI = nby == 1 ? by : by - 1, planesI = nbzHere == 1 ? bz : bz - 1;
+            const long long Cmax = rowsI * gx;
+            if (Cmax > FX_RES_THREADS) continue;
+            const long long parts = std::max(1LL, FX_RES_THREADS / std::max(1LL, Cmax));
+            const long long zlen = (planesI + parts - 1) / parts;
+            if (zlen > FX_RES_MAXZ) continue;
+            if (zlen < 4) continue;  // short columns: the faces-first variants do better (measured)
+            const long long F = 2LL * (by + bz) * gx;
+            work = (double)zlen + (double)((F + FX_RES_THREADS - 1) / FX_RES_THREADS);
+        } else if (variant != 0) {
             // faces (at most 2 (by + bz) rows of groups) and interior dealt out separately
             const int maxi = variant == 2 ? FX_RES_MAXI_SMALL : FX_RES_MAXI;
             if (2LL * (by + bz) * gx > (long long)FX_RES_MAXF * FX_RES_THREADS) continue;
@@ -600,7 +616,7 @@ struct firex_batch {
             // the faces-first variant (its small-box instance first) when every member fits
             // it, else the column variant
             const int cap = fx_res_capacity(members[0]->half);
-            for (int v : {2, 1, 0}) {
+            for (int v : {3, 2, 1, 0}) {
                 if (res_assign(dims, cap, v, &boxes, &resSmem)) {
                     resOk = true;
                     resVariant = v;

@@ -37,6 +37,7 @@
 #define FX_RES_MAXF 4                 // face groups per thread, faces-first variant
 #define FX_RES_MAXI 11                // interior groups per thread, faces-first variant
 #define FX_RES_MAXI_SMALL 7           // ... its instance for small boxes (fewer registers)
+#define FX_RES_MAXZ 10                // interior planes per thread column, faces-first column variant
 #define FX_RES_SMEM_MAX (226 * 1024)  // dynamic shared memory per CTA (227 KB opt-in less static)
 #define FX_RES_SPIN_LIMIT (1u << 24)  // polls of a neighbour's flag (well over a second with back-off)
 #define FX_RES_MAX_CTAS 1024          // boxes per simulation and phase (flag slots)
@@ -438,5 +439,186 @@ FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phas
         if (last) break;
         if (!fx_res_wait(cx.flags, cx.nb, (unsigned)s, cx.err, &s_flag)) return;
         fx_res_halo<PT>(cx, pout);
+    }
+}
+
+// Faces-first column variant: the face groups are dealt out over all threads as in the
+// faces-first variant and kept in registers (no parking); the interior is walked in z
+// columns, thread t taking interior column (x group, row) t with its z neighbours in
+// registers, its x neighbours from the adjacent lanes (warp shuffles) where those hold
+// the same row and plane.
+// Three CTA barriers per sweep: face stores done (then the flag), old values read and
+// neighbour flags seen (the waiting threads spin before it), new values and halo rows
+// written. For boxes whose interior columns fit the threads (planner: at most
+// FX_RES_MAXZ planes per column part).
+template <typename PT, bool ROUND>
+FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
+    __shared__ int s_flag;
+    const FxResCtx cx = fx_res_setup<PT>(S, bx, b, phase, sm);
+    const int n = cx.n, X = cx.X, Y = cx.Y, Z = cx.Z, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, gx = cx.gx;
+    const int rowsP = cx.rowsP;
+    const long long XY = cx.XY;
+    const bool nbLoY = cx.nbLoY, nbHiY = cx.nbHiY, nbLoZ = cx.nbLoZ, nbHiZ = cx.nbHiZ;
+    const int T = blockDim.x, t = threadIdx.x, lane = t & 31;
+    float* sp = cx.sp;
+    const float* sd = cx.sd;
+    const int planeP = rowsP * X, planeD = bx.by * X;
+    // ---- face groups, as in fx_res_box_early
+    const int fy0 = nbLoY ? 0 : -1, fy1 = (nbHiY && !(ny == 1 && nbLoY)) ? ny - 1 : -1;
+    const int fz0 = nbLoZ ? 0 : -1, fz1 = (nbHiZ && !(nz == 1 && nbLoZ)) ? nz - 1 : -1;
+    const int nyf = (fy0 >= 0) + (fy1 >= 0), nzf = (fz0 >= 0) + (fz1 >= 0);
+    const int lyA = nbLoY ? 1 : 0, nyi = max(0, (nbHiY ? ny - 1 : ny) - lyA);
+    const int lzA = nbLoZ ? 1 : 0, nzi = max(0, (nbHiZ ? nz - 1 : nz) - lzA);
+    const int FY = nyf * nz * gx, F = FY + nzf * nyi * gx;
+    int pf[FX_RES_MAXF];
+#pragma unroll
+    for (int k = 0; k < FX_RES_MAXF; ++k) {
+        const int i = t + k * T;
+        int q = 0, ly = 0, lz = 0;
+        if (i < FY) {
+            q = i % gx;
+            const int r = i / gx;
+            lz = r % nz;
+            ly = (r / nz == 0 && fy0 >= 0) ? fy0 : fy1;
+        } else if (i < F) {
+            const int j = i - FY;
+            q = j % gx;
+            const int r = j / gx;
+            ly = lyA + r % nyi;
+            lz = (r / nyi == 0 && fz0 >= 0) ? fz0 : fz1;
+        }
+        pf[k] = i < F ? (q | (ly << 10) | (lz << 21)) : -1;
+    }
+    // ---- this thread's interior column: (q, ly) = column t % C, z part t / C
+    const int C = nyi * gx;
+    const int P = C > 0 ? max(1, T / C) : 1;
+    const int zlen = (nzi + P - 1) / P;
+    const int col = C > 0 ? t % C : 0, part = C > 0 ? t / C : P;
+    const int q = col % gx, ly = lyA + col / gx, x0 = 4 * q;
+    const int zs = lzA + part * zlen;
+    const int cnt = part < P ? max(0, min(zlen, lzA + nzi - zs)) : 0;
+    const int y = y0 + ly;
+    const bool top = y == Y - 1;  // the open top is the ambient-pressure boundary
+    const int offC = ((zs + 1) * rowsP + ly + 1) * X + x0;  // (x0, ly, zs)
+    const int offD = (zs * bx.by + ly) * X + x0;
+    const int offB = y > 0 ? -X : 0;
+    const bool hasL = x0 > 0, hasR = x0 + 4 < X;
+    // x neighbours from the adjacent lane when it holds the adjacent group of the same
+    // row and z part (it then walks the same planes); else from shared memory
+    const bool shflL = lane > 0 && q > 0 && col > 0 && part < P;
+    const bool shflR = lane < 31 && q < gx - 1 && col < C - 1 && t + 1 < T && part < P;
+    const long long gRow = (long long)(z0 + zs) * XY + (long long)y * X + x0;
+    const FxJacobiConst2 c2 = fx_jacobi_const2(FxJacobiConst{S.jc[0], S.jc[1], S.jc[2], S.jc[3]}, S.jcRcp, S.jcFastDiv != 0);
+    // new value of face group g from the old values in shared memory
+    auto update = [&](int g) {
+        const int fq = g & 0x3ff, fly = (g >> 10) & 0x7ff, flz = g >> 21;
+        const int fyy = y0 + fly, fz = z0 + flz, fx0 = 4 * fq;
+        if (fyy == Y - 1) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float* rowC = sp + ((flz + 1) * rowsP + fly + 1) * X;
+        const float4 pc = *reinterpret_cast<const float4*>(rowC + fx0);
+        const float pl = fx0 > 0 ? rowC[fx0 - 1] : pc.x;
+        const float pr = fx0 + 4 < X ? rowC[fx0 + 4] : pc.w;
+        const float4 pb = *reinterpret_cast<const float4*>((fyy > 0 ? rowC - X : rowC) + fx0);
+        const float4 pt = *reinterpret_cast<const float4*>(rowC + X + fx0);
+        const float4 pkv = *reinterpret_cast<const float4*>((fz > 0 ? rowC - planeP : rowC) + fx0);
+        const float4 pfv = *reinterpret_cast<const float4*>((fz < Z - 1 ? rowC + planeP : rowC) + fx0);
+        const float4 d = *reinterpret_cast<const float4*>(sd + (flz * bx.by + fly) * X + fx0);
+        float4 o = fx_jacobi4(c2, pl, pc, pr, pb, pt, pkv, pfv, d);
+        if (ROUND) o = make_float4(PStore<__half>::round(o.x), PStore<__half>::round(o.y), PStore<__half>::round(o.z),
+                                   PStore<__half>::round(o.w));
+        return o;
+    };
+    auto gidx = [&](int g) {
+        const int fq = g & 0x3ff, fly = (g >> 10) & 0x7ff, flz = g >> 21;
+        return (z0 + flz) * XY + (long long)(y0 + fly) * X + 4 * fq;
+    };
+    auto sidx = [&](int g) {
+        const int fq = g & 0x3ff, fly = (g >> 10) & 0x7ff, flz = g >> 21;
+        return ((flz + 1) * rowsP + fly + 1) * X + 4 * fq;
+    };
+    if (t == 0) s_flag = 1;
+    __syncthreads();
+
+    for (int s = 0; s < n; ++s) {
+        const bool last = s == n - 1;
+        const bool full = s >= n - 2;  // the last two sweeps fill both buffers of the pair
+        void* pout = fx_solve_bufs(S, phase, s).pout;
+        float4 nf[FX_RES_MAXF];
+#pragma unroll
+        for (int k = 0; k < FX_RES_MAXF; ++k) {
+            if (pf[k] >= 0) {
+                nf[k] = update(pf[k]);
+                if (!last) PStore<PT>::st4(pout, gidx(pf[k]), nf[k]);
+            }
+        }
+        if (!last) {
+            __syncthreads();  // every face store of this CTA precedes the flag (release is cumulative)
+            if (t == 0) fx_st_release_u32(cx.flags + b, (unsigned)s + 1);
+        }
+        float4 nv[FX_RES_MAXZ];
+        {
+            float4 pc = make_float4(0.0f, 0.0f, 0.0f, 0.0f), pk = pc;  // threads without a column load nothing
+            if (cnt > 0) {
+                pc = *reinterpret_cast<const float4*>(sp + offC);
+                pk = (z0 + zs > 0) ? *reinterpret_cast<const float4*>(sp + offC - planeP) : pc;
+            }
+#pragma unroll
+            for (int k = 0; k < FX_RES_MAXZ; ++k) {
+                const bool v = k < cnt;
+                const int off = offC + k * planeP;
+                float4 pfv = pc;
+                if (v && z0 + zs + k < Z - 1) pfv = *reinterpret_cast<const float4*>(sp + off + planeP);
+                // every lane takes part in the shuffles; a value is used only from a lane of
+                // the same row and part, which walks the same plane k
+                const float fromL = __shfl_up_sync(0xffffffffu, pc.w, 1);
+                const float fromR = __shfl_down_sync(0xffffffffu, pc.x, 1);
+                if (v) {
+                    const float4 pb = *reinterpret_cast<const float4*>(sp + off + offB);
+                    const float4 pt = *reinterpret_cast<const float4*>(sp + off + X);
+                    const float pl = shflL ? fromL : (hasL ? sp[off - 1] : pc.x);
+                    const float pr = shflR ? fromR : (hasR ? sp[off + 4] : pc.w);
+                    const float4 d = *reinterpret_cast<const float4*>(sd + offD + k * planeD);
+                    float4 o = fx_jacobi4(c2, pl, pc, pr, pb, pt, pk, pfv, d);
+                    if (ROUND) o = make_float4(PStore<__half>::round(o.x), PStore<__half>::round(o.y),
+                                               PStore<__half>::round(o.z), PStore<__half>::round(o.w));
+                    nv[k] = top ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : o;
+                }
+                pk = pc;
+                pc = pfv;
+            }
+        }
+        // the neighbours' faces of this sweep: the waiting threads spin before the barrier
+        // that also ends every read of the old values
+        if (!last && t < 4 && cx.nb[t] >= 0) {
+            unsigned spins = 0;
+            while (fx_ld_acquire_u32(cx.flags + cx.nb[t]) < (unsigned)s + 1) {
+                if (++spins > FX_RES_SPIN_LIMIT) {
+                    atomicExch(cx.err, 1u);
+                    s_flag = 0;
+                    break;
+                }
+                if (spins > 64) __nanosleep(32);
+            }
+        }
+        __syncthreads();
+        if (!s_flag) return;  // a wait expired (every thread sees it after the barrier)
+        {
+#pragma unroll
+            for (int k = 0; k < FX_RES_MAXZ; ++k) {
+                if (k < cnt) {
+                    *reinterpret_cast<float4*>(sp + offC + k * planeP) = nv[k];
+                    if (full) PStore<PT>::st4(pout, gRow + (long long)k * XY, nv[k]);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < FX_RES_MAXF; ++k) {
+            if (pf[k] >= 0) {
+                *reinterpret_cast<float4*>(sp + sidx(pf[k])) = nf[k];
+                if (last) PStore<PT>::st4(pout, gidx(pf[k]), nf[k]);
+            }
+        }
+        if (last) break;
+        fx_res_halo<PT>(cx, pout);  // ends with the barrier before the next sweep
     }
 }

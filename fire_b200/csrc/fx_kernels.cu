@@ -588,7 +588,8 @@ __global__ void __launch_bounds__(256) fxk_norm_partial(const FxSimDev* __restri
 }
 
 // ---- every sweep of a Jacobi phase in one cooperative launch (fx_jacobi_res.cuh) --------
-// VARIANT: 0 column, 1 faces-first, 2 faces-first for small boxes (fx_jacobi_res.cuh).
+// VARIANT: 0 column, 1 faces-first, 2 faces-first for small boxes, 3 faces-first with
+// interior columns (fx_jacobi_res.cuh).
 template <typename PT, int VARIANT>
 __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatchDev* __restrict__ B, int phase) {
     extern __shared__ float4 fx_res_smem[];
@@ -601,6 +602,7 @@ __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatc
     const int b = w - B->start[FX_SHAPE_RES][si];
     if (VARIANT == 1) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI>(S, B->res[si], b, phase, sm);
     else if (VARIANT == 2) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI_SMALL>(S, B->res[si], b, phase, sm);
+    else if (VARIANT == 3) fx_res_box_v3<PT, sizeof(PT) == 2>(S, B->res[si], b, phase, sm);
     else fx_res_box_col<PT, sizeof(PT) == 2>(S, B->res[si], b, phase, sm);
 }
 
@@ -752,14 +754,18 @@ static const void* res_fn() {
     return (const void*)fxk_jacobi_res<PT, VARIANT>;
 }
 static const void* res_kernel(bool half, int variant) {
-    if (half) return variant == 1 ? res_fn<__half, 1>() : (variant == 2 ? res_fn<__half, 2>() : res_fn<__half, 0>());
-    return variant == 1 ? res_fn<float, 1>() : (variant == 2 ? res_fn<float, 2>() : res_fn<float, 0>());
+    switch (variant) {
+        case 1: return half ? res_fn<__half, 1>() : res_fn<float, 1>();
+        case 2: return half ? res_fn<__half, 2>() : res_fn<float, 2>();
+        case 3: return half ? res_fn<__half, 3>() : res_fn<float, 3>();
+        default: return half ? res_fn<__half, 0>() : res_fn<float, 0>();
+    }
 }
 
 // Largest resident-Jacobi grid that one cooperative launch can keep resident.
 int fx_res_capacity(bool half) {
     int cap = 1 << 30;
-    for (int variant = 0; variant < 3; ++variant) {  // every variant: the plan picks one later
+    for (int variant = 0; variant < 4; ++variant) {  // every variant: the plan picks one later
         const void* fn = res_kernel(half, variant);
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX) != cudaSuccess) {
             cudaGetLastError();

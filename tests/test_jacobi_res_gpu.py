@@ -2,7 +2,10 @@
 pressure held in shared memory, box faces exchanged through L2): its fields must be
 bit-identical to one sweep per launch in every branch (warm f32, cold f32, f16 storage
 rounded every sweep, mixed storage), for any sweep counts, grids that do and do not
-divide into boxes, and batches whose members share the launch."""
+divide into boxes, and batches whose members share the launch. The grids cover every
+variant the planner picks: faces first (small boxes), and faces first with interior
+columns, one column per thread (128x192x128, 80x120x80) or columns split in z parts
+(96x144x96)."""
 from __future__ import annotations
 
 import numpy as np
@@ -37,7 +40,7 @@ def pair(dims, opts, steps=3):
 
 
 @pytest.mark.parametrize("mode", [A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32, A.PRESSURE_F16])
-@pytest.mark.parametrize("dims", [(16, 20, 24), (36, 44, 28), (132, 20, 40), (64, 96, 64)])
+@pytest.mark.parametrize("dims", [(16, 20, 24), (36, 44, 28), (132, 20, 40), (64, 96, 64), (96, 144, 96), (80, 120, 80)])
 def test_resident_equals_single_sweeps(dims, mode):
     one, res = pair(dims, sphere_options(dims, P=12, R=9, pressure_mode=mode))
     same(one, res)
