@@ -616,7 +616,13 @@ struct firex_batch {
             // the faces-first variant (its small-box instance first) when every member fits
             // it, else the column variant
             const int cap = fx_res_capacity(members[0]->half);
+            // FX_RES_VARIANT (0-3) restricts the choice to one variant (tuning override)
+            static const int forced = [] {
+                const char* e = getenv("FX_RES_VARIANT");
+                return (e && e[0] >= '0' && e[0] <= '3' && !e[1]) ? e[0] - '0' : -1;
+            }();
             for (int v : {3, 2, 1, 0}) {
+                if (forced >= 0 && v != forced) continue;
                 if (res_assign(dims, cap, v, &boxes, &resSmem)) {
                     resOk = true;
                     resVariant = v;
