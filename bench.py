@@ -49,7 +49,7 @@ L2_BYTES = 126 * 1024 * 1024
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each Jacobi
 # kernel on this workload, from one ncu capture each (profiles/jacobi_*_hd.md).
-JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25258496 + 415232}
+JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25244416 + 621824}
 
 JACOBI_KERNEL_NAMES = {1: "fxk_jacobi<float>", 2: "fxk_jacobi_zm<float>", 3: "fxk_jacobi_tb<float>",
                        4: "fxk_jacobi_res<float>"}
