@@ -146,7 +146,8 @@ class Diagnostics(C.Structure):
         ("graph", C.c_int32),
         ("launches_per_step", C.c_int32),
         ("jacobi_kernel", C.c_int32),
-        ("reserved", C.c_int32 * 10),
+        ("jacobi_variant", C.c_int32),
+        ("reserved", C.c_int32 * 9),
     ]
 
 

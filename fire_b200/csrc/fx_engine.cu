@@ -604,8 +604,9 @@ struct firex_batch {
         tableDirty = true;
     }
 
-    // Fills the brick prefix sums for the launch shape (k, zc).
-    void fill_table(int k, int zc, int zmZc, bool wantRes) {
+    // Fills the brick prefix sums for the launch shape (k, zc); resident boxes when wanted,
+    // of variant resForce when that is 0-3.
+    void fill_table(int k, int zc, int zmZc, bool wantRes, int resForce) {
         int acc[FX_NSHAPES] = {};
         h->nsims = (int)members.size();
         std::vector<FxResBox> boxes;
@@ -613,16 +614,11 @@ struct firex_batch {
         if (wantRes && !members.empty()) {
             std::vector<std::array<int, 3>> dims;
             for (firex_sim* s : members) dims.push_back({s->X, s->Y, s->Z});
-            // the faces-first variant (its small-box instance first) when every member fits
-            // it, else the column variant
+            // the first variant every member fits: faces first with interior columns (long
+            // columns only), faces first (small-box instance first), then the column variant
             const int cap = fx_res_capacity(members[0]->half);
-            // FX_RES_VARIANT (0-3) restricts the choice to one variant (tuning override)
-            static const int forced = [] {
-                const char* e = getenv("FX_RES_VARIANT");
-                return (e && e[0] >= '0' && e[0] <= '3' && !e[1]) ? e[0] - '0' : -1;
-            }();
             for (int v : {3, 2, 1, 0}) {
-                if (forced >= 0 && v != forced) continue;
+                if (resForce >= 0 && v != resForce) continue;
                 if (res_assign(dims, cap, v, &boxes, &resSmem)) {
                     resOk = true;
                     resVariant = v;
@@ -658,7 +654,7 @@ struct firex_batch {
         tableK = k;
         tableZc = zc;
         tableZmZc = zmZc;
-        tableRes = wantRes ? 1 : 0;
+        tableRes = wantRes ? 2 + resForce : 0;
         tableWater = water_signature();
         tableDirty = true;
     }
@@ -688,6 +684,7 @@ struct firex_batch {
         const bool own = jacobiKernel != FIREX_JACOBI_AUTO;
         int kernel = own ? jacobiKernel : members[0]->jacobiKernel;
         int k = own ? jacobiK : members[0]->jacobiK;
+        const int resForce = (kernel == FIREX_JACOBI_RESIDENT && k >= 1) ? k - 1 : -1;  // block = variant + 1
         int zc = own ? jacobiZc : members[0]->jacobiZc;
         int dzc = 32;
         // AUTO and RESIDENT try the resident launch first; the single-sweep default is
@@ -707,9 +704,9 @@ struct firex_batch {
         if (!p.fuseP && !p.fuseR) p.k = 1;
         p.row4 = kernel == FIREX_JACOBI_UNBLOCKED;
         p.zmZc = (kernel == FIREX_JACOBI_ZMARCH && zc > 0) ? zc : zm_chunk(zm32, zm16);
-        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 1 : 0) ||
+        if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 2 + resForce : 0) ||
             tableWater != water_signature())
-            fill_table(p.k, p.zc, p.zmZc, wantRes);
+            fill_table(p.k, p.zc, p.zmZc, wantRes, resForce);
         p.res = wantRes && resOk;
         if (p.res) {
             p.resSmem = resSmem;
@@ -1569,18 +1566,24 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
         8 + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
+    out->jacobi_variant = p.res ? p.resVariant : -1;
     return FIREX_OK;
 }
 
 static bool jacobi_args_ok(int32_t kernel, int32_t block, int32_t zchunk) {
     if (kernel < FIREX_JACOBI_AUTO || kernel > FIREX_JACOBI_RESIDENT || zchunk < 0 || zchunk > 4096) return false;
+    if (kernel == FIREX_JACOBI_RESIDENT) return block >= 0 && block <= 4;
     return kernel != FIREX_JACOBI_FUSED || block == 2 || block == 3 || block == 4 || block == 6;
+}
+// the block argument kept per kernel: sweeps per launch (FUSED), variant + 1 (RESIDENT)
+static int jacobi_block_kept(int32_t kernel, int32_t block) {
+    return (kernel == FIREX_JACOBI_FUSED || kernel == FIREX_JACOBI_RESIDENT) ? block : 1;
 }
 
 int firex_set_jacobi(firex_sim* s, int32_t kernel, int32_t block, int32_t zchunk) {
     if (!s || !jacobi_args_ok(kernel, block, zchunk)) return FIREX_ERR_BAD_ARG;
     s->jacobiKernel = kernel;
-    s->jacobiK = kernel == FIREX_JACOBI_FUSED ? block : 1;
+    s->jacobiK = jacobi_block_kept(kernel, block);
     s->jacobiZc = zchunk;
     return FIREX_OK;
 }
@@ -1588,7 +1591,7 @@ int firex_set_jacobi(firex_sim* s, int32_t kernel, int32_t block, int32_t zchunk
 int firex_batch_set_jacobi(firex_batch* b, int32_t kernel, int32_t block, int32_t zchunk) {
     if (!b || !jacobi_args_ok(kernel, block, zchunk)) return FIREX_ERR_BAD_ARG;
     b->jacobiKernel = kernel;
-    b->jacobiK = kernel == FIREX_JACOBI_FUSED ? block : 1;
+    b->jacobiK = jacobi_block_kept(kernel, block);
     b->jacobiZc = zchunk;
     return FIREX_OK;
 }

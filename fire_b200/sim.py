@@ -270,17 +270,18 @@ class FireXSim(_Handle):
 
     @property
     def pressure_mode(self) -> int:
-        o = A.Options()
-        self._check(self._lib.firex_get_info(self._h, None, C.byref(o)))
-        return o.pressure_mode
+        o, d = A.Options(), A.DIMS()
+        self._check(self._lib.firex_get_info(self._h, d, C.byref(o)))
+        return o.pressure_mode  # the resolved branch (AUTO picked by grid size)
 
     @property
     def stream(self) -> int:
         return self._lib.firex_stream(self._h) or 0
 
-    def set_jacobi(self, kernel, block: int = 1, zchunk: int = 0) -> None:
-        """Jacobi kernel: 'auto', 'unblocked', 'zmarch' or 'fused' (with `block` sweeps per
-        launch), and z planes per CTA (0 = auto)."""
+    def set_jacobi(self, kernel, block: int = 0, zchunk: int = 0) -> None:
+        """Jacobi kernel: 'auto', 'unblocked', 'zmarch', 'fused' (with `block` sweeps per
+        launch) or 'resident' (`block` = box variant + 1, 0 = planner's choice), and z planes
+        per CTA (0 = auto)."""
         self._check(self._lib.firex_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
 
     @property
@@ -352,7 +353,7 @@ class FireXBatch:
     def step(self, n: int = 1, dt: float = 1.0 / 60.0) -> None:
         self._check(self._lib.firex_batch_step(self._h, int(n), float(dt)))
 
-    def set_jacobi(self, kernel, block: int = 1, zchunk: int = 0) -> None:
+    def set_jacobi(self, kernel, block: int = 0, zchunk: int = 0) -> None:
         self._check(self._lib.firex_batch_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
 
     def sync(self) -> None:

@@ -324,7 +324,9 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
 #define FIREX_JACOBI_FUSED 3
 /* Every sweep of a phase in one cooperative launch with the pressure held in shared
  * memory (only box faces cross L2 between sweeps); used by AUTO whenever the batch fits
- * on chip, else the single-sweep default runs. */
+ * on chip, else the single-sweep default runs. With RESIDENT, `block` 1-4 restricts the
+ * box plan to variant block - 1 (0 columns, 1 faces first, 2 faces first for small
+ * boxes, 3 faces first with interior columns); 0 lets the planner choose. */
 #define FIREX_JACOBI_RESIDENT 4
 int firex_set_jacobi(firex_sim* sim, int32_t kernel, int32_t block, int32_t zchunk);
 int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, int32_t zchunk);
@@ -337,7 +339,8 @@ typedef struct firex_diagnostics {
     int32_t graph;            /* 1: steps replay a captured CUDA graph */
     int32_t launches_per_step;
     int32_t jacobi_kernel;    /* FIREX_JACOBI_* kernel the last step ran */
-    int32_t reserved[10];
+    int32_t jacobi_variant;   /* RESIDENT: the box variant (0-3) it ran; else -1 */
+    int32_t reserved[9];
 } firex_diagnostics;
 int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
 
