@@ -5,10 +5,10 @@ Every Jacobi kernel of the library computes each sweep with the same FP32 operat
 the same order (the GPU tests hold them bit-identical), so the steps taken while tuning are
 ordinary steps of the run: the trajectory is the same whichever candidate ran them. The
 candidates are the resident kernel in each box variant that fits, the single-sweep kernels
-(unblocked, and z-marching with 8, 16 or 32 planes per CTA) and the fused kernel with 2 or
-4 sweeps per launch. The winner is applied with set_jacobi and remembered per workload
-signature (grid sizes, sweep counts, precision, pressure branch), optionally in a JSON file
-so that a later process starts tuned.
+(unblocked, and z-marching with 8, 16 or 32 planes per CTA) and the fused kernels (two
+sweeps per pass with 16-, 32- or 64-plane chunks, four sweeps per launch). The winner is
+applied with set_jacobi and remembered per workload signature (grid sizes, sweep counts,
+precision, pressure branch), optionally in a JSON file so that a later process starts tuned.
 """
 from __future__ import annotations
 
@@ -37,7 +37,8 @@ def default_candidates() -> list:
     out = [Candidate("resident", v + 1) for v in (3, 2, 1, 0)]
     out += [Candidate("unblocked")]
     out += [Candidate("zmarch", 0, zc) for zc in (8, 16, 32)]
-    out += [Candidate("fused", k, zc) for k in (2, 4) for zc in (8, 16)]
+    out += [Candidate("fused", 2, zc) for zc in (16, 32, 64)]
+    out += [Candidate("fused", 4, zc) for zc in (8, 16)]
     return out
 
 

@@ -26,6 +26,7 @@
 #include "fx_jacobi_res.cuh"
 #include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
+#include "fx_jacobi_zm2.cuh"
 
 namespace {
 
@@ -192,11 +193,14 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
 
 // Jacobi kernel when the caller did not choose one (measured on B200, 96+96 sweeps):
 // below 16 Mi cells per batch the unblocked kernel wins (the data stays in L2 and more
-// CTAs hide latency); above it the z-marching kernel with 32-plane chunks reaches 85-90 %
-// of the measured HBM copy bandwidth. fire_b200/autotune.py refines this per workload.
-void default_jacobi(long long cells, int* kernel, int* zc) {
-    *kernel = cells >= (16LL << 20) ? FIREX_JACOBI_ZMARCH : FIREX_JACOBI_UNBLOCKED;
-    *zc = 32;
+// CTAs hide latency); above it two sweeps per pass by z-marching tiles with 64-plane
+// chunks (the fused kernel with block 2): at 508^3, 50.8 ms of Jacobi per step against
+// 60.0 ms for one sweep per pass. fire_b200/autotune.py refines this per workload.
+void default_jacobi(long long cells, int* kernel, int* k, int* zc) {
+    const bool big = cells >= (16LL << 20);
+    *kernel = big ? FIREX_JACOBI_FUSED : FIREX_JACOBI_UNBLOCKED;
+    *k = big ? 2 : 1;
+    *zc = big ? 64 : 32;
 }
 
 // Box decomposition of an X x Y x Z grid over at most m CTAs for the resident Jacobi
@@ -644,7 +648,7 @@ struct firex_batch {
             acc[FX_SHAPE_TAB] += (fx_tab_layout(s->X, s->Y, s->Z).total + 255) / 256;
             acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z);
             acc[FX_SHAPE_ROW4] += (int)bricks_row4(s->X, s->Y, s->Z);
-            acc[FX_SHAPE_COL] += k > 1 ? fx_tb_bricks(s->X, s->Y, s->Z, k, zc) : 0;
+            acc[FX_SHAPE_COL] += k == 2 ? fx_zm2_bricks(s->X, s->Y, s->Z, zc) : (k > 1 ? fx_tb_bricks(s->X, s->Y, s->Z, k, zc) : 0);
             acc[FX_SHAPE_ZM] += fx_zm_bricks(s->X, s->Y, s->Z, zmZc);
         }
         for (int j = 0; j < FX_NSHAPES; ++j) {
@@ -686,11 +690,15 @@ struct firex_batch {
         int k = own ? jacobiK : members[0]->jacobiK;
         const int resForce = (kernel == FIREX_JACOBI_RESIDENT && k >= 1) ? k - 1 : -1;  // block = variant + 1
         int zc = own ? jacobiZc : members[0]->jacobiZc;
-        int dzc = 32;
-        // AUTO and RESIDENT try the resident launch first; the single-sweep default is
-        // the fallback when the batch does not fit on chip
+        // AUTO and RESIDENT try the resident launch first; the default is the fallback when
+        // the batch does not fit on chip
         const bool wantRes = kernel == FIREX_JACOBI_AUTO || kernel == FIREX_JACOBI_RESIDENT;
-        if (kernel == FIREX_JACOBI_AUTO || kernel == FIREX_JACOBI_RESIDENT) default_jacobi(cells, &kernel, &dzc);
+        if (kernel == FIREX_JACOBI_AUTO || kernel == FIREX_JACOBI_RESIDENT) {
+            int dk = 1, dzc = 32;
+            default_jacobi(cells, &kernel, &dk, &dzc);
+            k = dk;
+            if (zc <= 0) zc = dzc;
+        }
         if (kernel != FIREX_JACOBI_FUSED || (k != 2 && k != 3 && k != 4 && k != 6)) k = 1;
         long long zm32 = 0, zm16 = 0;
         for (firex_sim* s : members) {

@@ -18,6 +18,7 @@
 #include "fx_sph.cuh"
 #include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
+#include "fx_jacobi_zm2.cuh"
 #include "fx_step_math.cuh"
 #include "fx_storage.cuh"
 
@@ -370,6 +371,24 @@ __global__ void __launch_bounds__(FX_TB_THREADS, 1) fxk_jacobi_tb(const FxBatchD
         const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
         fx_tb_column<K, PT, ROUND>(S, bufs.pin, bufs.pout, bufs.zeroIn, tx, ty, z0, z1, sm, dsm);
         __syncthreads();  // the planes are reused by the next brick
+    });
+}
+
+// ---- two Jacobi sweeps per pass by z-marching tiles (fx_jacobi_zm2.cuh) ------------------------
+template <typename PT, bool ROUND>
+__global__ void __launch_bounds__(FX_Z2_THREADS, 2) fxk_jacobi_zm2(const FxBatchDev* __restrict__ B, int phase, int launch,
+                                                                int zc) {
+    extern __shared__ __align__(16) unsigned char fx_z2_dyn[];
+    FxZ2Smem<PT>& sm = *reinterpret_cast<FxZ2Smem<PT>*>(fx_z2_dyn);
+    fx_for_bricks<FX_SHAPE_COL>(B, [&](const FxSimDev& S, int b) {
+        const int ntx = (S.X + FX_Z2_TX - 1) / FX_Z2_TX, nty = (S.Y + FX_Z2_TY - 1) / FX_Z2_TY;
+        const int tx = b % ntx, ty = (b / ntx) % nty, zci = b / (ntx * nty);
+        const int z0 = zci * zc, z1 = min(S.Z, z0 + zc);
+        const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
+        const PT* pin = reinterpret_cast<const PT*>(bufs.pin);
+        PT* pout = reinterpret_cast<PT*>(bufs.pout);
+        if (bufs.zeroIn) fx_zm2_tile<PT, true, ROUND>(S, pin, pout, tx * FX_Z2_TX, ty * FX_Z2_TY, z0, z1, sm);
+        else fx_zm2_tile<PT, false, ROUND>(S, pin, pout, tx * FX_Z2_TX, ty * FX_Z2_TY, z0, z1, sm);
     });
 }
 
@@ -739,9 +758,26 @@ static void launch_tb_k(cudaStream_t s, int pmode, const FxBatchDev* B, int bric
     else launch_tb<K, __half, false>(s, B, bricks, phase, launch, zc);
 }
 
+template <typename PT, bool ROUND>
+static void launch_zm2(cudaStream_t s, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
+    static int g = [] {
+        cudaFuncSetAttribute((const void*)fxk_jacobi_zm2<PT, ROUND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(FxZ2Smem<PT>));
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fxk_jacobi_zm2<PT, ROUND>, FX_Z2_THREADS,
+                                                      sizeof(FxZ2Smem<PT>));
+        return (per_sm > 0 ? per_sm : 1) * num_sms();
+    }();
+    fxk_jacobi_zm2<PT, ROUND><<<bricks < g ? bricks : g, FX_Z2_THREADS, sizeof(FxZ2Smem<PT>), s>>>(B, phase, launch, zc);
+}
+
 bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
     switch (k) {
-        case 2: launch_tb_k<2>(s, pmode, B, bricks, phase, launch, zc); return true;
+        case 2:  // two sweeps per pass: the z-marching form
+            if (pmode == FX_TB_F32) launch_zm2<float, false>(s, B, bricks, phase, launch, zc);
+            else if (pmode == FX_TB_F16_ROUND) launch_zm2<__half, true>(s, B, bricks, phase, launch, zc);
+            else launch_zm2<__half, false>(s, B, bricks, phase, launch, zc);
+            return true;
         case 3: launch_tb_k<3>(s, pmode, B, bricks, phase, launch, zc); return true;
         case 4: launch_tb_k<4>(s, pmode, B, bricks, phase, launch, zc); return true;
         case 6: launch_tb_k<6>(s, pmode, B, bricks, phase, launch, zc); return true;

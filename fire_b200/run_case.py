@@ -1,7 +1,8 @@
 """Runs one simulation for a few steps and prints its diagnostics and per-pass times.
 
     python -m fire_b200.run_case X Y Z [--steps N] [--jacobi auto|unblocked|zmarch|fused|resident]
-                                       [--pressure auto|warm_f32|f16|cold_f32] [--mixed] [--iters P R]
+                                       [--block K] [--zchunk ZC] [--pressure auto|warm_f32|f16|cold_f32]
+                                       [--mixed] [--iters P R]
 
 A sphere emitter near the floor (radius X/9), seeded velocity noise and emission jitter,
 dt = 1/60. Used as the command under profilers (one process, one GPU, small cases).
@@ -23,6 +24,8 @@ def main() -> None:
     ap.add_argument("dims", type=int, nargs=3)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--jacobi", default="auto")
+    ap.add_argument("--block", type=int, default=0, help="fused sweeps per launch / resident variant + 1")
+    ap.add_argument("--zchunk", type=int, default=0, help="z planes per CTA (0 = auto)")
     ap.add_argument("--pressure", default="warm_f32", choices=list(PRESSURE))
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--iters", type=int, nargs=2, default=(96, 96))
@@ -34,7 +37,7 @@ def main() -> None:
                         precision=A.PRECISION_MIXED if a.mixed else A.PRECISION_F32,
                         spheres=[dict(center=(X / 2, Y / 16, Z / 2), radius=X / 9)])
     s = FireXSim((X, Y, Z), opts)
-    s.set_jacobi(a.jacobi)
+    s.set_jacobi(a.jacobi, a.block, a.zchunk)
     if a.profile:
         s.set_profiling(True)
         s.pass_times()

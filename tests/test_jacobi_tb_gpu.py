@@ -1,7 +1,10 @@
 """GPU tests of the temporally blocked Jacobi: K sweeps fused per launch must give
 bit-identical fields to K single-sweep launches in every FP32-arithmetic branch
 (warm f32, cold f32, f16 storage rounded every sweep), for grids that do and do not
-divide into the column tiles, any z chunking, and inside batches."""
+divide into the column tiles, any z chunking, and inside batches. K = 2 runs the
+two-sweep z-marching kernel (32 x 32 tiles with a one-cell ring; grids below, at and
+above one tile in x and y, chunks of 1 plane up to more than the grid), larger K the
+2.5-D column kernel."""
 from __future__ import annotations
 
 import numpy as np
@@ -25,8 +28,8 @@ def same(a, b):
 
 
 @pytest.mark.parametrize("mode", [A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32, A.PRESSURE_F16])
-@pytest.mark.parametrize("k,zc", [(2, 16), (3, 5), (4, 16), (4, 64), (6, 7)])
-@pytest.mark.parametrize("dims", [(16, 20, 24), (36, 44, 28), (64, 96, 64)])
+@pytest.mark.parametrize("k,zc", [(2, 1), (2, 16), (2, 33), (3, 5), (4, 16), (4, 64), (6, 7)])
+@pytest.mark.parametrize("dims", [(16, 20, 24), (36, 44, 28), (64, 96, 64), (132, 20, 40)])
 def test_fused_sweeps_equal_single_sweeps(dims, k, zc, mode):
     P = R = 12 if k != 3 else 9
     opts = sphere_options(dims, P=P, R=R, pressure_mode=mode)
@@ -38,11 +41,12 @@ def test_fused_sweeps_equal_single_sweeps(dims, k, zc, mode):
     same(one, fused)
 
 
-def test_fused_zero_dt_step_matches_oracle_bit_exact():
+@pytest.mark.parametrize("k", [2, 4])
+def test_fused_zero_dt_step_matches_oracle_bit_exact(k):
     dims = (36, 44, 28)
     opts = sphere_options(dims, P=16, R=12)
     g, o = FireXSim(dims, opts), OracleSim(dims, opts)
-    g.set_jacobi("fused", 4, 8)
+    g.set_jacobi("fused", k, 8)
     g.step(3, 0.0)
     o.step(3, 0.0)
     same(g, o)
@@ -61,7 +65,8 @@ def test_parity_rule_falls_back_to_single_sweeps():
     same(one, fused)
 
 
-def test_fused_batch_equals_single_sweep_alone():
+@pytest.mark.parametrize("k", [2, 4])
+def test_fused_batch_equals_single_sweep_alone(k):
     dims = [(64, 96, 64), (32, 48, 32), (36, 44, 28)]
     alone = [FireXSim(d, sphere_options(d, P=12, R=12, seed=i)) for i, d in enumerate(dims)]
     mixed = [FireXSim(d, sphere_options(d, P=12, R=12, seed=i)) for i, d in enumerate(dims)]
@@ -69,7 +74,7 @@ def test_fused_batch_equals_single_sweep_alone():
         s.set_jacobi("unblocked")
         s.step(3, DT)
     with FireXBatch() as b:
-        b.set_jacobi("fused", 4, 16)
+        b.set_jacobi("fused", k, 16)
         for s in mixed:
             b.add(s)
         b.step(3, DT)
