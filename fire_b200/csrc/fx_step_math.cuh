@@ -82,7 +82,9 @@ FXD float4 fx_trilinear(const FxGrid& g, const FxTri& t, Load load) {
 // Terms of simulate that depend only on time and on one or two coordinates are computed
 // once per step into a per-simulation table by fxk_step_tables, with the same device
 // expressions the per-cell code would evaluate (so results are bit-identical):
-//   uniform : exp(-dt*0.075/persistence), exp(-dt*0.14/persistence), pow(T_amb, 4)
+//   uniform : exp(-dt*0.075/persistence), exp(-dt*0.14/persistence), pow(T_amb, 4), and
+//             every other per-step constant of the cell update (metric, mixing weights,
+//             fire power and its root, clamped controls, the spray direction)
 //   x       : swirl z term, burner cellular/lobe/radial x terms
 //   y       : height envelope, outflow, outflow decay, outflow mix, burner vertical term
 //   z       : swirl x term, burner cellular/lobe/radial z terms
@@ -91,7 +93,16 @@ FXD float4 fx_trilinear(const FxGrid& g, const FxTri& t, Load load) {
 struct FxTabLayout {
     int x, y, z, ltx, lty, ltz, pulse, total;
 };
-enum { TU_DECAY_Z = 0, TU_DECAY_W = 1, TU_TAMB4 = 2, TU_COUNT = 8 };
+enum {
+    TU_DECAY_Z = 0, TU_DECAY_W, TU_TAMB4,
+    TU_MX, TU_MY, TU_MZ,                           // metric (shaders.ts:39-41)
+    TU_VMIX, TU_TMIX, TU_SMIX,                     // diffusion weights of velocity, T, species
+    TU_POWER, TU_POWER_ROOT, TU_THERMAL,           // firePower, sqrt, thermal power
+    TU_LIFT, TU_ENTRAIN, TU_AMB_O2, TU_HEAT,       // clamped lift, entrainment, ambient O2, heat release
+    TU_VORT_S, TU_TURB, TU_BUOY, TU_CINE,          // vorticity step, turbulence gain, clamped buoyancy, cinematic
+    TU_SPRAY_X, TU_SPRAY_Y, TU_SPRAY_Z,            // unit spray direction
+    TU_COUNT = 24
+};
 enum { TX_SWZ = 0, TX_CELL = 1, TX_LOBE = 2, TX_RAD = 3, TX_COUNT = 4 };
 enum { TY_HE = 0, TY_OUT = 1, TY_DECAY = 2, TY_MIX = 3, TY_VERT = 4, TY_COUNT = 5 };
 enum { TZ_SWX = 0, TZ_CELL = 1, TZ_LOBE = 2, TZ_RAD = 3, TZ_COUNT = 4 };
@@ -133,9 +144,40 @@ FXD float fx_table_entry(const float* u, int X, int Y, int Z, int i) {
     const float persistence = fx_clamp(u[U_PERSISTENCE], FC(0.4), 3.0f);
     auto nrm = [](int c, float dim) { return ((float)c + 0.5f) / dim; };
     if (i < L.x) {
-        if (i == TU_DECAY_Z) return expf(-dt * FC(0.075) / persistence);
-        if (i == TU_DECAY_W) return expf(-dt * FC(0.14) / persistence);
-        if (i == TU_TAMB4) return powf(u[U_T_AMBIENT], 4.0f);
+        const float3 m = fx_metric(u);
+        const float firePower = fx_clamp(u[U_FIRE_POWER], FC(0.1), 4.0f);
+        const float powerRoot = sqrtf(firePower);
+        switch (i) {
+            case TU_DECAY_Z: return expf(-dt * FC(0.075) / persistence);
+            case TU_DECAY_W: return expf(-dt * FC(0.14) / persistence);
+            case TU_TAMB4: return powf(u[U_T_AMBIENT], 4.0f);
+            case TU_MX: return m.x;
+            case TU_MY: return m.y;
+            case TU_MZ: return m.z;
+            case TU_VMIX: return fx_clamp(dt * FC(0.32), 0.0f, FC(0.12));
+            case TU_TMIX: return fx_clamp(dt * FC(0.18), 0.0f, FC(0.08));
+            case TU_SMIX: return fx_clamp(dt * FC(0.12), 0.0f, FC(0.06));
+            case TU_POWER: return firePower;
+            case TU_POWER_ROOT: return powerRoot;
+            case TU_THERMAL: return fx_min(powerRoot, 1.0f + FC(0.22) * (powerRoot - 1.0f));
+            case TU_LIFT: return fx_clamp(u[U_LIFT], 0.0f, 4.0f);
+            case TU_ENTRAIN: return fx_clamp(u[U_ENTRAIN], 0.0f, 3.0f);
+            case TU_AMB_O2: return fx_max(u[U_OXYGEN], FC(0.001));
+            case TU_HEAT: return 2150.0f + 1450.0f * u[U_HEAT_EFF];
+            case TU_VORT_S: return FC(0.00135) * u[U_VORTICITY] * dt;
+            case TU_TURB: return FC(0.075) + FC(0.16) * u[U_VORTICITY];
+            case TU_BUOY: return fx_clamp(u[U_BUOYANCY], 0.0f, 4.0f);
+            case TU_CINE: return fx_clamp(u[U_CINEMATIC], 0.0f, 1.0f);
+            default: break;
+        }
+        if (i >= TU_SPRAY_X && i <= TU_SPRAY_Z) {  // spray momentum direction (shaders.ts:293-297)
+            const float3 ext = fx_extent(u);
+            const float ox = FC(0.035) * ext.x, oy = FC(0.50) * ext.y, oz = FC(0.5) * ext.z;
+            const float tx = FC(0.52) * ext.x, ty = u[U_AIM_HEIGHT] * ext.y, tz = FC(0.5) * ext.z;
+            const float dx = tx - ox, dy = ty - oy, dz = tz - oz;
+            const float l = fx_length3(dx, dy, dz);
+            return i == TU_SPRAY_X ? dx / l : (i == TU_SPRAY_Y ? dy / l : dz / l);
+        }
         return 0.0f;
     }
     if (i < L.y) {
@@ -213,7 +255,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     float dt = u[U_DT];
 
     float4 orig = a.flow(id);
-    float3 metric = fx_metric(u);
+    const float3 metric = make_float3(__ldg(tab + TU_MX), __ldg(tab + TU_MY), __ldg(tab + TU_MZ));
     float btx = picx - orig.x * dt * metric.x;
     float bty = picy - orig.y * dt * metric.y;
     float btz = picz - orig.z * dt * metric.z;
@@ -235,12 +277,12 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         float vax = fx_divc(left.x + right.x + bottom.x + top.x + back.x + front.x, dc[DIVC_SIX]);
         float vay = fx_divc(left.y + right.y + bottom.y + top.y + back.y + front.y, dc[DIVC_SIX]);
         float vaz = fx_divc(left.z + right.z + bottom.z + top.z + back.z + front.z, dc[DIVC_SIX]);
-        float vm = fx_clamp(dt * FC(0.32), 0.0f, FC(0.12));
+        float vm = __ldg(tab + TU_VMIX);
         flow.x = fx_mix(flow.x, vax, vm);
         flow.y = fx_mix(flow.y, vay, vm);
         flow.z = fx_mix(flow.z, vaz, vm);
         float ta = fx_divc(left.w + right.w + bottom.w + top.w + back.w + front.w, dc[DIVC_SIX]);
-        flow.w = fx_mix(flow.w, ta, fx_clamp(dt * FC(0.18), 0.0f, FC(0.08)));
+        flow.w = fx_mix(flow.w, ta, __ldg(tab + TU_TMIX));
     }
     {  // species diffusion (shaders.ts:182-187)
         float4 sl = a.species(oL), sr = a.species(oR);
@@ -250,13 +292,13 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
                                  fx_divc(sl.y + sr.y + sb.y + st.y + sk.y + sf.y, dc[DIVC_SIX]),
                                  fx_divc(sl.z + sr.z + sb.z + st.z + sk.z + sf.z, dc[DIVC_SIX]),
                                  fx_divc(sl.w + sr.w + sb.w + st.w + sk.w + sf.w, dc[DIVC_SIX]));
-        species = fx_mix4(species, avg, fx_clamp(dt * FC(0.12), 0.0f, FC(0.06)));
+        species = fx_mix4(species, avg, __ldg(tab + TU_SMIX));
     }
 
     // Source injection (shaders.ts:189-201); the sphere list replaces the burner.
-    float firePower = fx_clamp(u[U_FIRE_POWER], FC(0.1), 4.0f);
-    float powerRoot = sqrtf(firePower);
-    float thermalPower = fx_min(powerRoot, 1.0f + FC(0.22) * (powerRoot - 1.0f));
+    const float firePower = __ldg(tab + TU_POWER);
+    const float powerRoot = __ldg(tab + TU_POWER_ROOT);
+    const float thermalPower = __ldg(tab + TU_THERMAL);
     float source;
     if (P.emitter_mode == FIREX_EMITTER_SPHERES) {
         source = 0.0f;
@@ -274,7 +316,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         const float cellular = FC(0.76) + FC(0.24) * __ldg(tab + L.x + TX_CELL * X + x) * __ldg(tab + L.z + TZ_CELL * Z + z);
         const float lobeArg = __ldg(tab + L.x + TX_LOBE * X + x) * __ldg(tab + L.z + TZ_LOBE * Z + z);
         const float lobes = fx_mix(FC(0.48), FC(1.18), fx_smoothstep_c(FC(-0.42), lobeArg, dc[DIVC_LOBE]));
-        const float texture = fx_mix(cellular, cellular * lobes, fx_clamp(u[U_CINEMATIC], 0.0f, 1.0f));
+        const float texture = fx_mix(cellular, cellular * lobes, __ldg(tab + TU_CINE));
         const float pulse = __ldg(tab + L.pulse + z * X + x);
         source = expf(-(radial + vertical)) * texture * pulse;
         species.x = fx_max(species.x, source * u[U_FUEL_RATE] * firePower);
@@ -288,7 +330,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         flow.x = flow.x + swx * s;
         flow.y = flow.y + swy * s;
         flow.z = flow.z + swz * s;
-        flow.y += source * dt * FC(0.52) * fx_clamp(u[U_LIFT], 0.0f, 4.0f) * powerRoot;
+        flow.y += source * dt * FC(0.52) * __ldg(tab + TU_LIFT) * powerRoot;
     }
 
     if (x == 0 || x == X - 1 || z == 0 || z == Z - 1 || y == Y - 1) {  // shaders.ts:203-208
@@ -310,8 +352,8 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     }
 
     // O2 entrainment (shaders.ts:220-232)
-    float entrainment = fx_clamp(u[U_ENTRAIN], 0.0f, 3.0f);
-    float ambientOxygen = fx_max(u[U_OXYGEN], FC(0.001));
+    const float entrainment = __ldg(tab + TU_ENTRAIN);
+    const float ambientOxygen = __ldg(tab + TU_AMB_O2);
     float oxygenDeficit = fx_clamp(fx_divc(ambientOxygen - species.y, dc[DIVC_AMBIENT_O2]), 0.0f, 1.0f);
     float fuelCore = fx_smoothstep_c(FC(0.30), species.x, dc[DIVC_FUELCORE]);
     float interfaceWeight = oxygenDeficit * fx_mix(1.0f, FC(0.18), fuelCore);
@@ -347,7 +389,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     species.y = fx_max(0.0f, oxygenBefore - burn * 4.0f);
     species.z = fx_clamp(species.z + burn * (1.0f + richness * FC(1.8)), 0.0f, 3.0f);
     species.w = fx_clamp(species.w + burn * FC(0.62), 0.0f, 3.0f);
-    flow.w += burn * (2150.0f + 1450.0f * u[U_HEAT_EFF]);
+    flow.w += burn * __ldg(tab + TU_HEAT);
     float reaction = fx_clamp(fx_divc(burn, dc[DIVC_DT]) * FC(0.22), 0.0f, 4.0f);
 
     {  // vorticity confinement: curl x grad(T) (shaders.ts:258-272)
@@ -361,7 +403,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         gx = gx / gl;
         gy = gy / gl;
         gz = gz / gl;
-        float vs = FC(0.00135) * u[U_VORTICITY] * dt;
+        const float vs = __ldg(tab + TU_VORT_S);
         flow.x = flow.x + (gy * cz - gz * cy) * vs;
         flow.y = flow.y + (gz * cx - gx * cz) * vs;
         flow.z = flow.z + (gx * cy - gy * cx) * vs;
@@ -372,31 +414,23 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         float ltx = __ldg(tab + L.ltx + z * Y + y);
         float lty = __ldg(tab + L.lty + z * X + x);
         float ltz = __ldg(tab + L.ltz + y * X + x);
-        float ts = (FC(0.075) + FC(0.16) * u[U_VORTICITY]) * hotPlume * heightEnvelope * dt;
+        float ts = __ldg(tab + TU_TURB) * hotPlume * heightEnvelope * dt;
         flow.x = flow.x + ltx * ts;
         flow.y = flow.y + lty * ts;
         flow.z = flow.z + ltz * ts;
     }
     {  // buoyancy (shaders.ts:287-288)
         float buoyancy = fx_clamp(fx_divc(flow.w - u[U_T_AMBIENT], dc[DIVC_BUOYANCY]), FC(-0.1), FC(1.2));
-        flow.y += buoyancy * dt * FC(0.72) * fx_clamp(u[U_BUOYANCY], 0.0f, 4.0f);
+        flow.y += buoyancy * dt * FC(0.72) * __ldg(tab + TU_BUOY);
     }
     if (liquidRaw) species.z *= expf(-water * dt * FC(4.8));  // exp(-0) == 1 exactly otherwise
     {  // spray momentum (shaders.ts:293-297)
-        float3 ext = fx_extent(u);
-        float ox = FC(0.035) * ext.x, oy = FC(0.50) * ext.y, oz = FC(0.5) * ext.z;
-        float tx = FC(0.52) * ext.x, ty = u[U_AIM_HEIGHT] * ext.y, tz = FC(0.5) * ext.z;
-        float dx = tx - ox, dy = ty - oy, dz = tz - oz;
-        float l = fx_length3(dx, dy, dz);
-        dx = dx / l;
-        dy = dy / l;
-        dz = dz / l;
+        const float dx = __ldg(tab + TU_SPRAY_X), dy = __ldg(tab + TU_SPRAY_Y), dz = __ldg(tab + TU_SPRAY_Z);
         flow.x = flow.x + dx * water * dt * FC(0.82);
         flow.y = flow.y + dy * water * dt * FC(0.82);
         flow.z = flow.z + dz * water * dt * FC(0.82);
     }
-    // radiation and decay (shaders.ts:299-304)
-    float persistence = fx_clamp(u[U_PERSISTENCE], FC(0.4), 3.0f);
+    // radiation and decay (shaders.ts:299-304); the decay factors come from the table
     // pow(T, 4): cells at exactly the ambient temperature (every cold cell clamped to it
     // above) take the per-step table value, which is the same powf of the same input
     const float tRad = fx_max(flow.w, 0.0f);
