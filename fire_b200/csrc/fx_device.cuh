@@ -17,7 +17,7 @@
 // Constant divisors of simulate. Each slot holds d > 0, rcp = RN(1/d) and the range
 // [lo, hi] of |x| where Markstein's correction step (fx_div_checked) reproduces IEEE
 // x / d; ok = 1 once the engine has checked that on the device for every float x.
-struct FxDivc {
+struct __align__(16) FxDivc {  // one 16-byte load brings d, rcp, lo and hi
     float d, rcp, lo, hi;
     int ok, pad[3];
 };
