@@ -494,7 +494,9 @@ def run_serve(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 300 for the HD step, as the reference's HD configuration; "
+                         "10 for batch48)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fire_b200", choices=["fire_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -503,6 +505,8 @@ def main() -> None:
                          "vs plain FP32; serve: Poisson-arrival serving")
     ap.add_argument("--serve-seconds", type=float, default=30.0)
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 10 if args.workload == "batch48" else 300
     if args.warmup < 3 and args.impl != "reference":
         args.warmup = 3
     if args.impl == "reference":
