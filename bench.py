@@ -56,6 +56,8 @@ JACOBI_KERNEL_NAMES = {1: "fxk_jacobi<float>", 2: "fxk_jacobi_zm<float>", 3: "fx
 
 
 def jacobi_kernel_name(diag: dict) -> str:
+    if diag.get("jacobi_kernel") == 3 and diag.get("jacobi_block") == 2:
+        return "fxk_jacobi_zm2<float>"  # two sweeps per pass
     return JACOBI_KERNEL_NAMES.get(diag.get("jacobi_kernel"), "fxk_jacobi<float>")
 
 
