@@ -94,3 +94,17 @@ def test_z_marching_and_unblocked_single_sweeps_agree(zc):
         a.step(3, DT)
         b.step(3, DT)
         same(a, b)
+
+
+def test_auto_runs_two_sweeps_per_pass_on_large_grids():
+    """At 16 Mi cells and above AUTO streams two sweeps per HBM pass (64-plane chunks);
+    the result equals single sweeps bit for bit."""
+    dims = (256, 256, 256)
+    opts = sphere_options(dims, P=8, R=4)
+    auto, one = FireXSim(dims, opts), FireXSim(dims, opts)
+    one.set_jacobi("zmarch")
+    auto.step(2, DT)
+    one.step(2, DT)
+    d = auto.diagnostics
+    assert d["jacobi_kernel"] == A.JACOBI_FUSED and d["jacobi_block"] == 2 and d["jacobi_zchunk"] == 64, d
+    same(auto, one)
