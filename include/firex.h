@@ -313,10 +313,13 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
  *   UNBLOCKED — one thread per 4 cells, neighbours through L1 (best for small grids);
  *   ZMARCH    — x-y tiles marching z through a cp.async shared-memory ring (one read of
  *               each value per sweep: best once the grid outgrows L2);
- *   FUSED     — `block` sweeps per launch (2, 3, 4 or 6), temporally blocked. Fused sweeps
- *               give the same results as single sweeps except that mixed precision keeps
- *               the intermediate sweeps in FP32. A phase falls back to single sweeps when
- *               fusing would change which buffer holds the result.
+ *   FUSED     — `block` sweeps per launch (2, 3, 4 or 6), temporally blocked: block 2 is
+ *               the two-sweep z-marching pass (one read of pressure and divergence per two
+ *               sweeps; AUTO's choice at 16 Mi cells and above), 3, 4 and 6 the 2.5-D
+ *               column kernel. Fused sweeps give the same results as single sweeps (with
+ *               FP16 pressure storage the intermediate sweeps are rounded as stored ones).
+ *               A phase falls back to single sweeps when fusing would change which buffer
+ *               holds the result.
  * `zchunk`: z planes per CTA for ZMARCH and FUSED (0 = auto). AUTO picks by grid size. */
 #define FIREX_JACOBI_AUTO 0
 #define FIREX_JACOBI_UNBLOCKED 1
