@@ -14,8 +14,8 @@
 // flight. Sweep 2 is the only value stored. The chunk's sweep-1 planes reach one plane past
 // it at each end, so each chunk is independent.
 //
-// Every update is the single sweep's FP32 computation (fx_jacobi4, or fx_jacobi_update
-// for single ring cells: both give the IEEE quotient), the open top row is 0 after each
+// Every update is the single sweep's FP32 computation (fx_jacobi4, or fx_jacobi1 for
+// single ring cells: both give the IEEE quotient), the open top row is 0 after each
 // sweep, and with FP16 storage the sweep-1 values are rounded to FP16 as a stored sweep
 // would be: two fused sweeps are bit-identical to two single sweeps. Boundaries follow the
 // reference's clamped addressing: input rows and planes are loaded clamped into the grid,
@@ -33,7 +33,14 @@
 #define FX_Z2_COLS 40        // slot row: 4-cell segment, 32 cells, 4-cell segment
 #define FX_Z2_PROWS 34       // input pressure rows: y0 - 2 .. y0 + 31
 #define FX_Z2_RROWS 32       // divergence and sweep-1 rows: y0 - 1 .. y0 + 30
-#define FX_Z2_SLOTS 7        // input and divergence rings: planes z - 2 .. z + 4 at step z
+#ifndef FX_Z2_SLOTS
+#define FX_Z2_SLOTS 6        // input and divergence rings: planes z - 2 .. z + SLOTS - 3 at step z
+#endif
+#define FX_Z2_AHEAD (FX_Z2_SLOTS - 3)  // step z issues the copies of plane z + AHEAD
+static_assert(FX_Z2_SLOTS >= 5, "planes z - 2 .. z + 2 must fit the rings");
+#ifndef FX_Z2_MINB
+#define FX_Z2_MINB 2         // CTAs per SM the registers are budgeted for
+#endif
 #define FX_Z2_SSLOTS 4       // sweep-1 ring: planes z - 3 .. z - 1 (read) and z (written)
 
 template <typename PT>
@@ -82,8 +89,7 @@ FXD FxZ2Plan fx_zm2_plan(int X, int Y, int x0, int y0) {
 
 template <typename PT>
 FXD void fx_zm2_issue(FxZ2Smem<PT>& sm, const FxZ2Plan& P, const PT* __restrict__ p, const float* __restrict__ div,
-                      long long XY, int Z, int q, bool loadP, bool withDiv) {
-    const int slot = (q + 2 * FX_Z2_SLOTS) % FX_Z2_SLOTS;
+                      long long XY, int Z, int q, int slot, bool loadP, bool withDiv) {
     const int qc = q < 0 ? 0 : (q > Z - 1 ? Z - 1 : q);
     const long long plane = (long long)qc * XY;
 #pragma unroll
@@ -108,7 +114,6 @@ FXD void fx_zm2_tile(const FxSimDev& S, const PT* __restrict__ pin, PT* __restri
     const long long XY = (long long)X * Y;
     const float* __restrict__ div = S.div;
     const FxJacobiConst2 c2 = fx_jacobi_const2(FxJacobiConst{S.jc[0], S.jc[1], S.jc[2], S.jc[3]}, S.jcRcp, S.jcFastDiv != 0);
-    const FxJacobiConst c1{S.jc[0], S.jc[1], S.jc[2], S.jc[3]};
     // this thread's group: 4 cells at (x0 + 4 cg, y0 - 1 + row); sweep-1 row `row` of the
     // ring, and for rows 1..30 the tile's row row - 1 in sweep 2
     const int t = threadIdx.x, cg = t & 7, row = t >> 3;
@@ -129,22 +134,25 @@ FXD void fx_zm2_tile(const FxSimDev& S, const PT* __restrict__ pin, PT* __restri
     const int prow = row + 1;              // its input row (input rows start at y0 - 2)
     const int o0 = row * FX_Z2_COLS + pcol;  // its offset in divergence and sweep-1 slots
 
-    for (int q = zs1 - 1; q <= zs1 + 3; ++q) {
-        fx_zm2_issue<PT>(sm, plan, pin, div, XY, Z, q, loadP, q >= zs1 && q <= ze1);
+    // ring slots: plane q lives in slot q mod 7 of the input and divergence rings and in
+    // slot q mod 4 (q & 3, q >= -2) of the sweep-1 ring; s0 tracks z mod 7 incrementally
+    int s0 = zs1 % FX_Z2_SLOTS;
+    for (int q = zs1 - 1; q <= zs1 + FX_Z2_AHEAD - 1; ++q) {
+        fx_zm2_issue<PT>(sm, plan, pin, div, XY, Z, q, (q + FX_Z2_SLOTS) % FX_Z2_SLOTS, loadP, q >= zs1 && q <= ze1);
         fx_cp_commit();
     }
     for (int z = zs1; z <= ze1 + 2; ++z) {
-        fx_cp_wait<2>();  // this thread's copies of planes up to z + 1 have landed
+        const int sm1 = s0 == 0 ? FX_Z2_SLOTS - 1 : s0 - 1, sp1 = s0 == FX_Z2_SLOTS - 1 ? 0 : s0 + 1;
+        fx_cp_wait<FX_Z2_AHEAD - 2>();  // this thread's copies of planes up to z + 1 have landed
         __syncthreads();  // ... everyone's; sweep-1 plane z - 1 is complete; every read of the
                           // slots refilled below (input and divergence plane z - 3) is done
         {
-            const int q = z + 4;
-            fx_zm2_issue<PT>(sm, plan, pin, div, XY, Z, q, loadP && q <= ze1 + 1, q <= ze1);
+            const int q = z + FX_Z2_AHEAD;
+            fx_zm2_issue<PT>(sm, plan, pin, div, XY, Z, q, s0 >= 3 ? s0 - 3 : s0 + FX_Z2_AHEAD, loadP && q <= ze1 + 1, q <= ze1);
             fx_cp_commit();
         }
         if (z <= ze1) {  // ---- sweep 1 on plane z
-            const int s0 = z % FX_Z2_SLOTS, sm1 = (z + FX_Z2_SLOTS - 1) % FX_Z2_SLOTS, sp1 = (z + 1) % FX_Z2_SLOTS;
-            float* out = sm.s[z % FX_Z2_SSLOTS];
+            float* out = sm.s[z & (FX_Z2_SSLOTS - 1)];
             // x neighbours from the adjacent lanes (the same row's groups cg - 1, cg + 1); the
             // row's end groups read the ring segments
             const float4 cen = in1 ? p4(s0, prow, pcol) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -168,8 +176,8 @@ FXD void fx_zm2_tile(const FxSimDev& S, const PT* __restrict__ pin, PT* __restri
                     const float c = p1(s0, hrow, hcol);
                     const float l = cx == 0 ? c : p1(s0, hrow, hcol - 1);
                     const float rr = cx == X - 1 ? c : p1(s0, hrow, hcol + 1);
-                    o = fx_jacobi_update(c1, l, rr, p1(s0, hrow - 1, hcol), p1(s0, hrow + 1, hcol), p1(sm1, hrow, hcol),
-                                         p1(sp1, hrow, hcol), sm.d[s0][srow * FX_Z2_COLS + hcol]);
+                    o = fx_jacobi1(c2, l, rr, p1(s0, hrow - 1, hcol), p1(s0, hrow + 1, hcol), p1(sm1, hrow, hcol),
+                                   p1(sp1, hrow, hcol), sm.d[s0][srow * FX_Z2_COLS + hcol]);
                     if (ROUND) o = PStore<__half>::round(o);
                 }
                 out[srow * FX_Z2_COLS + hcol] = o;
@@ -177,26 +185,27 @@ FXD void fx_zm2_tile(const FxSimDev& S, const PT* __restrict__ pin, PT* __restri
         }
         const int qz = z - 2;  // ---- sweep 2 on plane z - 2
         const bool do2 = qz >= z0 && qz < z1;  // uniform over the CTA
-        const float* s2 = sm.s[(qz + FX_Z2_SSLOTS) % FX_Z2_SSLOTS];
+        const float* s2 = sm.s[qz & (FX_Z2_SSLOTS - 1)];
         const float4 cen2 = do2 && in2 ? *reinterpret_cast<const float4*>(s2 + o0) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const float fromL2 = __shfl_up_sync(0xffffffffu, cen2.w, 1), fromR2 = __shfl_down_sync(0xffffffffu, cen2.x, 1);
         if (do2 && in2) {
             float4 o = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (y != Y - 1) {
-                const float* s0 = s2;
-                const float* sk = qz > 0 ? sm.s[(qz - 1) % FX_Z2_SSLOTS] : s0;
-                const float* sf = qz < Z - 1 ? sm.s[(qz + 1) % FX_Z2_SSLOTS] : s0;
+                const float* sk = qz > 0 ? sm.s[(qz - 1) & (FX_Z2_SSLOTS - 1)] : s2;
+                const float* sf = qz < Z - 1 ? sm.s[(qz + 1) & (FX_Z2_SSLOTS - 1)] : s2;
                 const float4 cen = cen2;
-                const float l = x == 0 ? cen.x : (cg > 0 ? fromL2 : s0[o0 - 1]);
-                const float rr = x + 3 == X - 1 ? cen.w : (cg < 7 ? fromR2 : s0[o0 + 4]);
-                const float4 b = y > 0 ? *reinterpret_cast<const float4*>(s0 + o0 - FX_Z2_COLS) : cen;
-                const float4 tt = *reinterpret_cast<const float4*>(s0 + o0 + FX_Z2_COLS);
-                const float4 dv = *reinterpret_cast<const float4*>(&sm.d[qz % FX_Z2_SLOTS][o0]);
+                const float l = x == 0 ? cen.x : (cg > 0 ? fromL2 : s2[o0 - 1]);
+                const float rr = x + 3 == X - 1 ? cen.w : (cg < 7 ? fromR2 : s2[o0 + 4]);
+                const float4 b = y > 0 ? *reinterpret_cast<const float4*>(s2 + o0 - FX_Z2_COLS) : cen;
+                const float4 tt = *reinterpret_cast<const float4*>(s2 + o0 + FX_Z2_COLS);
+                // divergence plane z - 2: slot (z - 2) mod 7
+                const float4 dv = *reinterpret_cast<const float4*>(&sm.d[s0 >= 2 ? s0 - 2 : s0 + FX_Z2_SLOTS - 2][o0]);
                 o = fx_jacobi4(c2, l, cen, rr, b, tt, *reinterpret_cast<const float4*>(sk + o0),
                                *reinterpret_cast<const float4*>(sf + o0), dv);
             }
             PStore<PT>::st4(pout, (long long)qz * XY + (long long)y * X + x, o);
         }
+        s0 = sp1;
     }
     fx_cp_wait<0>();
     __syncthreads();

@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(FX_TB_THREADS, 1) fxk_jacobi_tb(const FxBatchD
 
 // ---- two Jacobi sweeps per pass by z-marching tiles (fx_jacobi_zm2.cuh) ------------------------
 template <typename PT, bool ROUND>
-__global__ void __launch_bounds__(FX_Z2_THREADS, 2) fxk_jacobi_zm2(const FxBatchDev* __restrict__ B, int phase, int launch,
+__global__ void __launch_bounds__(FX_Z2_THREADS, FX_Z2_MINB) fxk_jacobi_zm2(const FxBatchDev* __restrict__ B, int phase, int launch,
                                                                 int zc) {
     extern __shared__ __align__(16) unsigned char fx_z2_dyn[];
     FxZ2Smem<PT>& sm = *reinterpret_cast<FxZ2Smem<PT>*>(fx_z2_dyn);

@@ -574,10 +574,10 @@ FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, floa
     const fx_f2 r01 = fx_fma2(fx_fma2(q01, c.negDenom, n01), c.rcp, q01);
     const fx_f2 r23 = fx_fma2(fx_fma2(q23, c.negDenom, n23), c.rcp, q23);
     const float2 ra = fx_unpack2(r01), rb = fx_unpack2(r23);
-    // every |x| inside [2^-96, FLT_MAX] (bit patterns 0x0f800000 .. 0x7f7fffff)?
-    const unsigned lo = 0x0f800000u, span = 0x7f7fffffu - 0x0f800000u;
-    const bool ok = ((__float_as_uint(a.x) & 0x7fffffffu) - lo <= span) & ((__float_as_uint(a.y) & 0x7fffffffu) - lo <= span) &
-                    ((__float_as_uint(b.x) & 0x7fffffffu) - lo <= span) & ((__float_as_uint(b.y) & 0x7fffffffu) - lo <= span);
+    // every |x| inside [2^-96, FLT_MAX]? (false for zeros, tiny x, infinities and NaN)
+    const float lo = 1.2621774483536189e-29f, hi = 3.402823466e38f;
+    const bool ok = (fabsf(a.x) >= lo) & (fabsf(a.x) <= hi) & (fabsf(a.y) >= lo) & (fabsf(a.y) <= hi) &
+                    (fabsf(b.x) >= lo) & (fabsf(b.x) <= hi) & (fabsf(b.y) >= lo) & (fabsf(b.y) <= hi);
     if (ok) return make_float4(ra.x, ra.y, rb.x, rb.y);
     return make_float4(fx_div_by_const(a.x, c.denom, c.rcpS), fx_div_by_const(a.y, c.denom, c.rcpS),
                        fx_div_by_const(b.x, c.denom, c.rcpS), fx_div_by_const(b.y, c.denom, c.rcpS));
@@ -585,5 +585,11 @@ FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, floa
 
 FXD float fx_jacobi_update(const FxJacobiConst& c, float l, float r, float b, float t, float k, float f, float div) {
     return __fdiv_rn(fx_jacobi_numerator(c, l, r, b, t, k, f, div), c.denom);
+}
+
+// One cell of fx_jacobi4 (the same numerator; the checked constant division when enabled).
+FXD float fx_jacobi1(const FxJacobiConst2& c, float l, float r, float b, float t, float k, float f, float div) {
+    const float n = fx_jacobi_numerator(FxJacobiConst{c.wxS, c.wyS, c.wzS, c.denom}, l, r, b, t, k, f, div);
+    return c.fast ? fx_div_by_const(n, c.denom, c.rcpS) : __fdiv_rn(n, c.denom);
 }
 
