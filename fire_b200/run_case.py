@@ -2,10 +2,12 @@
 
     python -m fire_b200.run_case X Y Z [--steps N] [--jacobi auto|unblocked|zmarch|fused|resident]
                                        [--block K] [--zchunk ZC] [--pressure auto|warm_f32|f16|cold_f32]
-                                       [--mixed] [--iters P R]
+                                       [--mixed] [--iters P R] [--profile] [--time N]
 
 A sphere emitter near the floor (radius X/9), seeded velocity noise and emission jitter,
 dt = 1/60. Used as the command under profilers (one process, one GPU, small cases).
+--time N then times N more steps as the engine runs them (graph replay) with CUDA events on
+the simulation's stream and prints their mean as step_ms.
 """
 from __future__ import annotations
 
@@ -30,6 +32,7 @@ def main() -> None:
     ap.add_argument("--mixed", action="store_true")
     ap.add_argument("--iters", type=int, nargs=2, default=(96, 96))
     ap.add_argument("--profile", action="store_true", help="per-pass device times (no graph replay)")
+    ap.add_argument("--time", type=int, default=0, help="then time this many steps (graph replay)")
     a = ap.parse_args()
     X, Y, Z = a.dims
     opts = make_options(pressure_iterations=a.iters[0], correction_iterations=a.iters[1], seed=1, velocity_noise=0.05,
@@ -46,6 +49,19 @@ def main() -> None:
     out = {"dims": [X, Y, Z], "steps": a.steps, "diagnostics": s.diagnostics}
     if a.profile:
         out["pass_ms"] = {k: v[0] / a.steps for k, v in s.pass_times().items()}
+        s.set_profiling(False)
+    if a.time > 0:
+        import torch
+
+        st = torch.cuda.ExternalStream(s.stream)
+        s.step(1, 1 / 60)  # plan and graph for the unprofiled step
+        s.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.step(a.time, 1 / 60)
+        e1.record(st)
+        s.sync()
+        out["step_ms"] = e0.elapsed_time(e1) / a.time
     print(json.dumps(out))
     s.close()
 
