@@ -44,3 +44,29 @@ def rel_l2(a, b, ref=None) -> float:
 def interior(a):
     """Interior cells (one-cell outer shell excluded), arrays shaped (Z, Y, X, ...)."""
     return a[1:-1, 1:-1, 1:-1]
+
+
+def config3_spheres(dims=(508, 508, 508), seed=0, n=3):
+    """The 508^3 configuration's emitters: ``n`` seeded spheres of radius 20-40 cells resting
+    near the floor, away from the side walls."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = dims
+    out = []
+    for _ in range(n):
+        r = float(rng.uniform(20.0, 40.0))
+        out.append(dict(center=(float(rng.uniform(r + 8, X - r - 8)), r + 4.0, float(rng.uniform(r + 8, Z - r - 8))),
+                        radius=r, fuel=1.0, temperature=1500.0))
+    return out
+
+
+def backward_divergence(flow, u):
+    """computeDivergence (shaders.ts:344-364) in float32 with the kernel's operation order:
+    (u - u[x-1]) mx + (v - v[y-1]) my + (w - w[z-1]) mz, clamped neighbours, metric =
+    grid / max(domain, 0.001) from the uniform block ``u``. ``flow`` is (Z, Y, X, 4)."""
+    f32 = np.float32
+    m = [f32(u[k]) / max(f32(u[32 + k]), f32(0.001)) for k in range(3)]
+    U, V, W = flow[..., 0], flow[..., 1], flow[..., 2]
+    left = np.concatenate([U[:, :, :1], U[:, :, :-1]], axis=2)
+    bottom = np.concatenate([V[:, :1], V[:, :-1]], axis=1)
+    back = np.concatenate([W[:1], W[:-1]], axis=0)
+    return ((U - left) * m[0] + (V - bottom) * m[1]) + (W - back) * m[2]
