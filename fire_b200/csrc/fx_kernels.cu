@@ -274,8 +274,10 @@ __global__ void __launch_bounds__(256) fxk_jacobi(const FxBatchDev* __restrict__
 // The solve's result sits in the buffer after its last launch; launch counts have the
 // parity of the sweep counts (the engine only fuses sweeps when they do), so the result
 // buffer is the reference's: p[(base + P) & 1] and corr[R & 1].
+// 8 CTAs per SM (32 registers, some spilled): 18 % faster than the 5 that 48 registers allow
+// at 508^3 (latency-bound: more loads in flight); the divergence kernel is fastest at 57.
 template <typename PT>
-__global__ void __launch_bounds__(256) fxk_project(const FxBatchDev* __restrict__ B, int phase) {
+__global__ void __launch_bounds__(256, 8) fxk_project(const FxBatchDev* __restrict__ B, int phase) {
     fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
         const Lane4 r = fx_lane4(S, b);
         if (r.n <= 0) return;
