@@ -320,7 +320,9 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
  *               FP16 pressure storage the intermediate sweeps are rounded as stored ones).
  *               A phase falls back to single sweeps when fusing would change which buffer
  *               holds the result.
- * `zchunk`: z planes per CTA for ZMARCH and FUSED (0 = auto). AUTO picks by grid size. */
+ * `zchunk`: z planes per CTA for ZMARCH and FUSED (0 = auto). AUTO takes RESIDENT when the
+ * batch fits on chip, else by its cell count: UNBLOCKED below 8 Mi cells, ZMARCH with
+ * 16-plane chunks below 16 Mi, FUSED with block 2 and 64-plane chunks from 16 Mi. */
 #define FIREX_JACOBI_AUTO 0
 #define FIREX_JACOBI_UNBLOCKED 1
 #define FIREX_JACOBI_ZMARCH 2
