@@ -583,10 +583,6 @@ FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, floa
                        fx_div_by_const(b.x, c.denom, c.rcpS), fx_div_by_const(b.y, c.denom, c.rcpS));
 }
 
-FXD float fx_jacobi_update(const FxJacobiConst& c, float l, float r, float b, float t, float k, float f, float div) {
-    return __fdiv_rn(fx_jacobi_numerator(c, l, r, b, t, k, f, div), c.denom);
-}
-
 // One cell of fx_jacobi4 (the same numerator; the checked constant division when enabled).
 FXD float fx_jacobi1(const FxJacobiConst2& c, float l, float r, float b, float t, float k, float f, float div) {
     const float n = fx_jacobi_numerator(FxJacobiConst{c.wxS, c.wyS, c.wzS, c.denom}, l, r, b, t, k, f, div);
