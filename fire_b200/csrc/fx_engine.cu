@@ -197,7 +197,7 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
 // it); from 8 Mi cells, where they outgrow L2, one sweep per pass by z-marching tiles
 // with 16-plane chunks (192x288x192: 6.48 ms per step against 7.52 unblocked); from
 // 16 Mi cells two sweeps per pass with 64-plane chunks (the fused kernel with block 2):
-// at 508^3, 47.7 ms of Jacobi per step against 54.5 ms for one sweep per pass.
+// at 508^3, 45.1 ms of Jacobi per step against 56.5 ms for one sweep per pass.
 // fire_b200/autotune.py refines this per workload.
 void default_jacobi(long long cells, int* kernel, int* k, int* zc) {
     const bool big = cells >= (16LL << 20), mid = !big && cells >= (8LL << 20);
