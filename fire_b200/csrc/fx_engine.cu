@@ -194,15 +194,15 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
 // Jacobi kernel when the caller did not choose one (measured on B200, 96+96 sweeps):
 // below 8 Mi cells per batch the unblocked kernel (the pressure pair and the divergence
 // stay in L2 and more CTAs hide latency; at 160x240x160 the z-marching kernel only ties
-// it); from 8 Mi cells, where they outgrow L2, one sweep per pass by z-marching tiles
-// with 16-plane chunks (192x288x192: 6.48 ms per step against 7.52 unblocked); from
-// 16 Mi cells two sweeps per pass with 64-plane chunks (the fused kernel with block 2):
-// at 508^3, 45.1 ms of Jacobi per step against 56.5 ms for one sweep per pass.
-// fire_b200/autotune.py refines this per workload.
+// it); from 8 Mi cells, where they outgrow L2, two sweeps per pass by z-marching tiles
+// (the fused kernel with block 2) with 16-plane chunks (192x288x192: 6.29 ms per step
+// against 6.48 with one sweep per pass and 7.52 unblocked), and from 16 Mi cells with
+// 64-plane chunks (508^3: 45.1 ms of Jacobi per step against 56.5 ms for one sweep per
+// pass). fire_b200/autotune.py refines this per workload.
 void default_jacobi(long long cells, int* kernel, int* k, int* zc) {
     const bool big = cells >= (16LL << 20), mid = !big && cells >= (8LL << 20);
-    *kernel = big ? FIREX_JACOBI_FUSED : (mid ? FIREX_JACOBI_ZMARCH : FIREX_JACOBI_UNBLOCKED);
-    *k = big ? 2 : 1;
+    *kernel = (big || mid) ? FIREX_JACOBI_FUSED : FIREX_JACOBI_UNBLOCKED;
+    *k = (big || mid) ? 2 : 1;
     *zc = big ? 64 : (mid ? 16 : 32);
 }
 

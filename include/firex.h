@@ -315,14 +315,14 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
  *               each value per sweep: best once the grid outgrows L2);
  *   FUSED     — `block` sweeps per launch (2, 3, 4 or 6), temporally blocked: block 2 is
  *               the two-sweep z-marching pass (one read of pressure and divergence per two
- *               sweeps; AUTO's choice at 16 Mi cells and above), 3, 4 and 6 the 2.5-D
+ *               sweeps; AUTO's choice at 8 Mi cells and above), 3, 4 and 6 the 2.5-D
  *               column kernel. Fused sweeps give the same results as single sweeps (with
  *               FP16 pressure storage the intermediate sweeps are rounded as stored ones).
  *               A phase falls back to single sweeps when fusing would change which buffer
  *               holds the result.
  * `zchunk`: z planes per CTA for ZMARCH and FUSED (0 = auto). AUTO takes RESIDENT when the
- * batch fits on chip, else by its cell count: UNBLOCKED below 8 Mi cells, ZMARCH with
- * 16-plane chunks below 16 Mi, FUSED with block 2 and 64-plane chunks from 16 Mi. */
+ * batch fits on chip, else by its cell count: UNBLOCKED below 8 Mi cells, FUSED with block 2
+ * and 16-plane chunks below 16 Mi, FUSED with block 2 and 64-plane chunks from 16 Mi. */
 #define FIREX_JACOBI_AUTO 0
 #define FIREX_JACOBI_UNBLOCKED 1
 #define FIREX_JACOBI_ZMARCH 2

@@ -96,8 +96,8 @@ def test_z_marching_and_unblocked_single_sweeps_agree(zc):
         same(a, b)
 
 
-def test_auto_marches_z_one_sweep_per_pass_between_8_and_16_mi_cells():
-    """From 8 Mi cells (past L2) to 16 Mi AUTO takes the z-marching kernel with 16-plane
+def test_auto_runs_two_sweeps_per_pass_with_short_chunks_between_8_and_16_mi_cells():
+    """From 8 Mi cells (past L2) to 16 Mi AUTO streams two sweeps per HBM pass in 16-plane
     chunks; the result equals the unblocked kernel's bit for bit."""
     dims = (192, 288, 192)
     opts = sphere_options(dims, P=6, R=5)
@@ -106,7 +106,7 @@ def test_auto_marches_z_one_sweep_per_pass_between_8_and_16_mi_cells():
     auto.step(2, DT)
     one.step(2, DT)
     d = auto.diagnostics
-    assert d["jacobi_kernel"] == A.JACOBI_ZMARCH and d["jacobi_zchunk"] == 16, d
+    assert d["jacobi_kernel"] == A.JACOBI_FUSED and d["jacobi_block"] == 2 and d["jacobi_zchunk"] == 16, d
     same(auto, one)
 
 
