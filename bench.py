@@ -45,10 +45,12 @@ METRIC = "Gcell-steps/s"
 WORKLOAD = "fire-x step, HD tier 128x192x128, plain FP32, sphere r=14 @ (64,12,64), +-10% jitter, 96+96 Jacobi, dt=1/60"
 JACOBI_BYTES_PER_CELL = 12  # read p + read div + write p, f32 (algorithmic, per sweep)
 L2_BYTES = 126 * 1024 * 1024
+E2E_MIN_STEPS = 200
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each Jacobi
-# kernel on this workload, from one ncu capture each (profiles/jacobi_*_hd.md).
+# kernel on this workload, from one ncu capture of that kernel (the same command as this
+# benchmark's default run, one launch captured).
 JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25244416 + 621824}
 
 JACOBI_KERNEL_NAMES = {1: "fxk_jacobi<float>", 2: "fxk_jacobi_zm<float>", 3: "fxk_jacobi_tb<float>",
@@ -80,29 +82,75 @@ def config(extra=None) -> dict:
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons during the timed region."""
+    """Samples SM clocks and clock-event (throttle) reasons during a timed region, through
+    NVML every 20 ms (reads only; nvidia-smi every 200 ms where NVML is unavailable)."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                   "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, device_index: int):
+    def __init__(self, device_index: int, interval_s: float = 0.02):
         self.idx = device_index
-        self.samples = []
+        self.pci = None  # the CUDA device's PCI address: NVML indices need not follow CUDA's
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(device_index)
+            self.pci = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        except Exception:
+            pass
+        self.interval = interval_s
+        self.samples = []  # (sm_mhz, max_mhz, set of active reason names)
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+
+    def _sample_nvml(self, h):
+        import pynvml as N
+        sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        bits = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+        return float(sm), float(mx), {k for k, b in self.REASON_BITS.items() if bits & b}
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", self.pci or str(self.idx), f"--query-gpu={self.QUERY}",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        parts = [p.strip() for p in out.stdout.strip().split(",")]
+        if len(parts) < 9:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        return float(parts[1]), float(parts[2]), {names[i] for i in range(4) if parts[5 + i].lower() == "active"}
 
     def _run(self):
-        while not self._stop.is_set():
+        h = None
+        try:
+            import pynvml as N
+            N.nvmlInit()
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.QUERY}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                parts = [p.strip() for p in out.stdout.strip().split(",")]
-                if len(parts) >= 9:
-                    self.samples.append(parts)
+                h = N.nvmlDeviceGetHandleByPciBusId(self.pci) if self.pci else None
+            except Exception:
+                h = None
+            if h is None:
+                h = N.nvmlDeviceGetHandleByIndex(self.idx)
+            self._nvml = N
+        except Exception:
+            h = None
+        while True:
+            try:
+                s = self._sample_nvml(h) if h is not None else self._sample_smi()
+                if s:
+                    self.samples.append(s)
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            if self._stop.wait(self.interval if h is not None else 0.2):
+                break
+        if self._nvml is not None:
+            try:
+                self._nvml.nvmlShutdown()
+            except Exception:
+                pass
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -116,13 +164,11 @@ class ClockSampler:
 
     def summary(self) -> dict:
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples),
+                "reasons": sorted(set().union(*(s[2] for s in self.samples))), "samples": len(self.samples),
+                "source": "nvml" if self._nvml is not None else "nvidia-smi"}
 
 
 def measured_peak_hbm() -> tuple[float, str]:
@@ -164,7 +210,7 @@ def run_reference(args) -> None:
     from oracle import oracle as O
     O.build()
     sim = O.OracleSim(DIMS, options(make_options))
-    for _ in range(min(args.warmup, 1)):
+    for _ in range(args.warmup):
         sim.step(1, DT)
     budget = float(os.environ.get("FIREX_REFERENCE_BUDGET_S", "90"))
     times = []
@@ -180,9 +226,10 @@ def run_reference(args) -> None:
     value = cells() * n / el / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": el / n * 1e3, "higher_is_better": True,
+        "steps": n, "warmup": args.warmup, "ms_per_step": el / n * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config({"reference_path": "CPU restatement of src/sim/firex WGSL step (oracle/firex_oracle.cpp)"}),
+        "config": config(),
+        "reference_path": "CPU restatement of the src/sim/firex WGSL step (oracle/firex_oracle.cpp), OpenMP",
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": O.num_threads(), "kind": "port",
                          "sample": f"{n} of {args.steps} requested HD steps (budget {budget:.0f} s)"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -251,11 +298,11 @@ def run_gpu(args) -> None:
     # ---- end-to-end through the C ABI with host buffers: every step's flow field is
     # copied into pinned host memory (firex_read_field_async: staged on the device in
     # stream order, then copied while the next step runs); the clock stops after the last
-    # copy has landed; as many steps as the device-timed region, so that the last copy's
-    # tail weighs on the rate as it does in a long run ----
+    # copy has landed; at least E2E_MIN_STEPS steps (a window of a few tens of ms on the
+    # host clock is dominated by its own start and stop) ----
     pinned = [torch.empty((DIMS[2], DIMS[1], DIMS[0], 4), dtype=torch.float32, pin_memory=True) for _ in range(2)]
     hosts = [p.numpy() for p in pinned]
-    e2e_steps = max(1, args.steps)
+    e2e_steps = max(E2E_MIN_STEPS, args.steps)
     sim.step(1, DT)
     sim.read_async("flow", hosts[0])
     sim.sync()
@@ -281,6 +328,12 @@ def run_gpu(args) -> None:
     kernel = jacobi_kernel_name(diag)
     traffic = JACOBI_TRAFFIC_PER_LAUNCH.get(kernel)
 
+    sim.close()
+    extra = {}
+    if world == 1 and not args.hd_only:
+        extra["config3_508"] = measure_508()
+        extra["batch48"] = measure_batch48(steps=BATCH48_DEFAULT_STEPS, warmup=3)
+
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -304,9 +357,9 @@ def run_gpu(args) -> None:
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            **extra,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
     reps.close()
 
 
@@ -333,40 +386,41 @@ def batch48_scenes(seed: int = 4242, count: int = 48):
     return out
 
 
-def run_batch48(args) -> None:
+def measure_batch48(steps: int, warmup: int = 3) -> dict:
     """Gcell-steps/s of the 48-simulation batch in mixed precision (one set of launches per
     step for all members, graph-replayed) against the same 48 simulations stepped one at a
     time in plain FP32, plus the post-projection divergence of every mixed member against
-    its plain FP32 twin (relative to the twin's pre-projection scale: the divergence of the
-    first step's predicted flow is not kept, so the plain post-projection norm is used)."""
+    its plain FP32 twin (relative to the twin's post-projection norm). The accuracy bar
+    itself (one step from the FP64 oracle's state, <= 1e-4 of the pre-projection norm) is
+    held by the GPU tests, which may run the oracle; this program times the GPU only."""
     import numpy as np
     import torch
 
     from fire_b200 import _abi as A
     from fire_b200.sim import FireXBatch, FireXSim, make_options
 
-    torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
     scenes = batch48_scenes()
-    steps = args.steps
     cells = [d[0] * d[1] * d[2] for d, _ in scenes]
     total_cells = sum(cells)
 
     # plain FP32, one simulation at a time (each on its own stream, its own step graph)
     plain_ms = 0.0
     plain_norms = []
-    for dims, o in scenes:
-        s = FireXSim(dims, make_options(**o))
-        st = torch.cuda.ExternalStream(s.stream)
-        s.step(args.warmup, DT)
-        s.sync()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        s.step(steps, DT)
-        e1.record(st)
-        s.sync()
-        plain_ms += e0.elapsed_time(e1)
-        plain_norms.append(s.read("final_divergence"))
-        s.close()
+    with ClockSampler(dev) as clk_plain:
+        for dims, o in scenes:
+            s = FireXSim(dims, make_options(**o))
+            st = torch.cuda.ExternalStream(s.stream)
+            s.step(warmup, DT)
+            s.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            s.step(steps, DT)
+            e1.record(st)
+            s.sync()
+            plain_ms += e0.elapsed_time(e1)
+            plain_norms.append(s.read("final_divergence"))
+            s.close()
     plain = total_cells * steps / (plain_ms / 1e3) / 1e9
 
     # batched, mixed precision; the Jacobi kernel and tiles are picked by the autotuner on a
@@ -385,14 +439,15 @@ def run_batch48(args) -> None:
     scratch, scratch_members = mixed_batch()
     tuner.tune(scratch, DT)
     scratch.close()
-    del scratch_members
+    for m in scratch_members:
+        m.close()
     b, members = mixed_batch()
     choice = tuner.tune(b, DT)  # cached: applied without stepping
     st = torch.cuda.ExternalStream(b.stream)
-    b.step(args.warmup, DT)
+    b.step(warmup, DT)
     b.sync()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
-    with ClockSampler(0) as clk:
+    with ClockSampler(dev) as clk:
         evs[0].record(st)
         for i in range(steps):
             b.step(1, DT)
@@ -403,32 +458,132 @@ def run_batch48(args) -> None:
     batched = total_cells * steps / (batch_ms / 1e3) / 1e9
     diag = members[0].diagnostics
     # drift: each mixed member's post-projection divergence field after the run against its
-    # plain FP32 twin's, relative to the twin's (post-projection) norm. Not the accuracy bar,
-    # which is one step from the same state against the FP64 oracle, relative to the
-    # pre-projection norm (the GPU parity tests); this shows how far FP16 species rounding
-    # moves a multi-step trajectory.
+    # plain FP32 twin's, relative to the twin's (post-projection) norm; it shows how far FP16
+    # species rounding moves a multi-step trajectory
     worst = 0.0
     for m, ref in zip(members, plain_norms):
         d = m.read("final_divergence")[1:-1, 1:-1, 1:-1].astype(np.float64)
         r = ref[1:-1, 1:-1, 1:-1].astype(np.float64)
         worst = max(worst, float(np.linalg.norm((d - r).ravel()) / max(np.linalg.norm(r.ravel()), 1e-300)))
     b.close()
-    line = {
-        "metric": "Gcell-steps/s batched mixed vs plain FP32", "value": batched, "unit": METRIC, "n_gpus": 1,
-        "steps": steps, "warmup": args.warmup, "ms_per_step": batch_ms / steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (species stored f16)", "data": "synthetic",
-        "config": {"workload": "48 simulations, grids by seed from 64x96x64 / 96x144x96 / 128x192x128 / 160x240x160, "
-                               "1-3 spheres r 6-24, 96+96 Jacobi, dt=1/60, Jacobi kernel and tiles autotuned",
-                   "cells": total_cells,
-                   "grids": {str(d): sum(1 for x, _ in scenes if x == d) for d in BATCH_FAMILY},
-                   "l2": "inputs larger than L2"},
-        "plain_fp32_sequential": plain, "speedup_vs_plain": batched / plain,
+    for m in members:
+        m.close()
+    return {
+        "workload": "48 simulations, grids by seed from 64x96x64 / 96x144x96 / 128x192x128 / 160x240x160, "
+                    "1-3 spheres r 6-24, 96+96 Jacobi, dt=1/60, species stored FP16 (batched) vs plain FP32 "
+                    "one simulation at a time, Jacobi kernel and tiles autotuned",
+        "cells": total_cells, "grids": {str(d): sum(1 for x, _ in scenes if x == d) for d in BATCH_FAMILY},
+        "steps": steps, "warmup": warmup,
+        "value": batched, "unit": METRIC, "ms_per_step": batch_ms / steps,
+        "plain_fp32_sequential": plain, "plain_ms_per_step": plain_ms / steps, "speedup_vs_plain": batched / plain,
         "p50_step_ms": percentile(step_ms, 0.5), "p99_step_ms": percentile(step_ms, 0.99),
         "jacobi_kernel": diag.get("jacobi_kernel"), "launches_per_step": diag.get("launches_per_step"),
         "jacobi_autotune": {"choice": choice.as_list(), "ms_per_step_by_candidate": tuner.last_timings},
-        "final_divergence_drift_vs_plain_max": worst, "clocks": clk.summary(),
+        "final_divergence_drift_vs_plain_max": worst,
+        "accuracy_bar": "rel_div <= 1e-4 vs the FP64 oracle, one step from its state (tests/test_mixed_gpu.py)",
+        "clocks": clk.summary(), "clocks_plain": clk_plain.summary(),
+    }
+
+
+def run_batch48(args) -> None:
+    import torch
+
+    torch.cuda.set_device(0)
+    r = measure_batch48(args.steps, args.warmup)
+    line = {
+        "metric": "Gcell-steps/s batched mixed vs plain FP32", "value": r["value"], "unit": METRIC, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (species stored f16)", "data": "synthetic",
+        "config": {"workload": r["workload"], "cells": r["cells"], "grids": r["grids"], "l2": "inputs larger than L2"},
+        **{k: v for k, v in r.items() if k not in ("workload", "cells", "grids", "value", "steps", "warmup",
+                                                  "ms_per_step", "unit")},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---- the 508^3 grid: plain FP32 (branch A), three seeded spheres near the floor ------------
+DIMS_508 = (508, 508, 508)
+STEPS_508 = 20
+# algorithmic bytes per cell of each pass of a 96 + 96 step (plain FP32, AoS flow, one sweep
+# per Jacobi iteration, copyFlow replaced by a parity flip): simulate 72, two divergences of
+# 20, 192 sweeps of 12, two projections of 36 = 2488 B per cell-step
+PASS_BYTES_PER_CELL = {"simulate": 72, "divergence": 2 * 20, "jacobi": 192 * 12, "project": 2 * 36}
+STEP_BYTES_PER_CELL = sum(PASS_BYTES_PER_CELL.values())
+BATCH48_DEFAULT_STEPS = 50
+
+
+def config3_spheres(seed: int = 0, n: int = 3):
+    """Three seeded spheres of radius 20-40 cells resting near the floor of the 508^3 grid,
+    away from the side walls."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    X, Y, Z = DIMS_508
+    out = []
+    for _ in range(n):
+        r = float(rng.uniform(20.0, 40.0))
+        out.append(dict(center=(float(rng.uniform(r + 8, X - r - 8)), r + 4.0, float(rng.uniform(r + 8, Z - r - 8))),
+                        radius=r, fuel=1.0, temperature=1500.0))
+    return out
+
+
+def measure_508(warmup: int = 3, steps: int = STEPS_508) -> dict:
+    """The 508^3 configuration in plain FP32 (branch A, warm-started FP32 pressure): device
+    time of `steps` graph-replayed steps with the HBM-roofline fraction of the whole step,
+    then the same steps pass by pass (CUDA events between passes) for the per-pass table."""
+    import torch
+
+    from fire_b200 import _abi as A
+    from fire_b200.sim import FireXSim, make_options
+
+    dev = torch.cuda.current_device()
+    sim = FireXSim(DIMS_508, make_options(pressure_iterations=96, correction_iterations=96, seed=0, velocity_noise=0.05,
+                                          emission_jitter=0.0, spheres=config3_spheres(),
+                                          pressure_mode=A.PRESSURE_WARM_F32))
+    st = torch.cuda.ExternalStream(sim.stream)
+    sim.step(warmup, DT)
+    sim.sync()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    with ClockSampler(dev) as clk:
+        evs[0].record(st)
+        for i in range(steps):
+            sim.step(1, DT)
+            evs[i + 1].record(st)
+        sim.sync()
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+    total_ms = evs[0].elapsed_time(evs[-1])
+    diag = sim.diagnostics
+    prof = 3
+    sim.set_profiling(True)
+    sim.pass_times()
+    sim.step(prof, DT)
+    passes = sim.pass_times()
+    sim.set_profiling(False)
+    sim.close()
+    n = DIMS_508[0] * DIMS_508[1] * DIMS_508[2]
+    peak, peak_kind = measured_peak_hbm()
+    ms = total_ms / steps
+    achieved = STEP_BYTES_PER_CELL * n / (ms / 1e3) / 1e9
+    per_pass = {}
+    for k, b in PASS_BYTES_PER_CELL.items():
+        t = passes[k][0] / prof
+        a = b * n / (t / 1e3) / 1e9 if t > 0 else None
+        per_pass[k] = {"ms_per_step": t, "launches_per_step": passes[k][1] / prof, "algorithmic_bytes_per_cell": b,
+                       "achieved_gbs": a, "frac": a / peak if a else None}
+    return {
+        "workload": "fire-x step, 508x508x508 (131,096,512 cells), plain FP32 (branch A), 3 seeded spheres r 20-40 "
+                    "near the floor, velocity noise +-0.05, 96+96 Jacobi, dt=1/60",
+        "cells": n, "steps": steps, "warmup": warmup,
+        "value": n * steps / (total_ms / 1e3) / 1e9, "unit": METRIC, "ms_per_step": ms,
+        "p50_step_ms": percentile(step_ms, 0.5), "p99_step_ms": percentile(step_ms, 0.99),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "bytes_per_cell_step": STEP_BYTES_PER_CELL,
+                     "target_frac": 0.70},
+        "passes": per_pass, "profiled_steps": prof,
+        "jacobi": {"kernel": jacobi_kernel_name(diag), "block": diag.get("jacobi_block"),
+                   "zchunk": diag.get("jacobi_zchunk")},
+        "launches_per_step": diag.get("launches_per_step"),
+        "clocks": clk.summary(),
+    }
 
 
 # ---- served stream: Poisson arrivals, admission by HBM budget, continuous batching -----------
@@ -507,6 +662,8 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fire_b200", choices=["fire_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--hd-only", action="store_true",
+                    help="the HD line alone, without the 508^3 and 48-simulation objects")
     ap.add_argument("--workload", default="hd", choices=["hd", "batch48", "serve"],
                     help="hd: the headline HD step (default); batch48: 48 uneven simulations, batched mixed "
                          "vs plain FP32; serve: Poisson-arrival serving")

@@ -20,6 +20,7 @@
 // not a device address. Its device address is looked up once per device with
 // cudaGetSymbolAddress, with that device current, on the first call that runs there;
 // that first call should come before any stream capture on the caller's side.
+#include <cuda.h>  // CUdeviceptr / CUresult, for the driver's address-range query
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -121,6 +122,23 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+// cuMemGetAddressRange through the runtime's driver entry point (no link-time dependency
+// on the driver library): the base and size of the allocation that holds a device address.
+using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
+AddressRangeFn address_range_fn() {
+    static AddressRangeFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<AddressRangeFn>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
 }  // namespace
 
 extern "C" int firex_divergence_norm_noalloc(const void* flow, const int32_t dims[3], const float metric[3],
@@ -146,6 +164,20 @@ extern "C" int firex_divergence_norm_noalloc(const void* flow, const int32_t dim
         return fail(FIREX_ERR_BAD_ARG, "flow is not device memory");
     }
     if (attr.device >= FX_NOALLOC_MAX_DEVICES) return fail(FIREX_ERR_UNSUPPORTED, "device ordinal above 63");
+    // The allocation that holds flow must hold every record the dims ask for: the kernels
+    // would otherwise read past its end.
+    const unsigned long long need = (unsigned long long)X * Y * Z * 16ull;
+    if (AddressRangeFn range = address_range_fn()) {
+        CUdeviceptr base = 0;
+        size_t size = 0;
+        const CUdeviceptr dp = (CUdeviceptr)(uintptr_t)attr.devicePointer;
+        if (range(&base, &size, dp) != CUDA_SUCCESS)
+            return fail(FIREX_ERR_BAD_ARG, "flow is not inside a device allocation");
+        if (dp - base > size || need > (unsigned long long)(size - (dp - base)))
+            return fail(FIREX_ERR_BAD_ARG, "dims need " + std::to_string(need) + " bytes of flow records; the allocation "
+                                           "holds " + std::to_string((unsigned long long)(size - (dp - base))) +
+                                           " from flow to its end");
+    }
     int prev = -1;
     e = cudaGetDevice(&prev);
     if (e == cudaSuccess && prev != attr.device) e = cudaSetDevice(attr.device);
@@ -154,6 +186,7 @@ extern "C" int firex_divergence_norm_noalloc(const void* flow, const int32_t dim
     if (e == cudaSuccess) {
         cudaStream_t st = static_cast<cudaStream_t>(stream);
         const int nPlanes = Z - 2;
+        cudaGetLastError();  // an earlier error of the caller's own work is not this call's
         fxk_noalloc_plane<<<nPlanes, 256, 0, st>>>(static_cast<const float4*>(attr.devicePointer), X, Y, metric[0],
                                                    metric[1], metric[2], scratch);
         fxk_noalloc_final<<<1, 256, 0, st>>>(scratch, nPlanes);

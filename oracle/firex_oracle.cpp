@@ -29,6 +29,11 @@
 // (correction) solve stored in FP16 as branch B stores it. The library does not offer it:
 // measured against the FP64 step it misses the 1e-4 divergence bar by about 40x.
 #define FXO_PRESSURE_WARM_F32_F16C 4
+// Oracle-only pressure branch for the precision study: the primary (warm-started) solve
+// stored in FP16 as branch B stores it, the divergence of the projected flow, the residual
+// (correction) solve and the final projection in FP32 (iterative refinement of the FP16
+// solve by the residual iterations).
+#define FXO_PRESSURE_F16P_F32C 5
 
 #include <algorithm>
 #include <cmath>
@@ -978,6 +983,9 @@ struct Sim : SimBase {
             if (mode == FXO_PRESSURE_WARM_F32_F16C) {
                 pressure[i].assign(N, T(0));
                 correction16[i].assign(N, 0);
+            } else if (mode == FXO_PRESSURE_F16P_F32C) {
+                pressure16[i].assign(N, 0);
+                correction[i].assign(N, T(0));
             } else if (mode == FIREX_PRESSURE_F16) {
                 pressure16[i].assign(N, 0);
                 correction16[i].assign(N, 0);
@@ -1096,6 +1104,24 @@ struct Sim : SimBase {
             project<T, uint16_t>(g, flow[0].data(), correction16[ci].data(), flow[1].data());
             lastCorrection = ci;
             lastCorrectionShared = false;
+        } else if (mode == FXO_PRESSURE_F16P_F32C) {  // FP16 primary solve, FP32 residual solve
+            for (int i = 0; i < P; ++i) {
+                jacobi_sweep<T, uint16_t>(g, pressure16[pressureIndex].data(), divergence.data(),
+                                          pressure16[1 - pressureIndex].data());
+                pressureIndex = 1 - pressureIndex;
+            }
+            project<T, uint16_t>(g, flow[1].data(), pressure16[pressureIndex].data(), flow[0].data());
+            divergence_pass(g, flow[0].data(), divergence.data());
+            std::fill(correction[0].begin(), correction[0].end(), T(0));
+            std::fill(correction[1].begin(), correction[1].end(), T(0));
+            int ci = 0;
+            for (int i = 0; i < R; ++i) {
+                jacobi_sweep<T, T>(g, correction[ci].data(), divergence.data(), correction[1 - ci].data());
+                ci = 1 - ci;
+            }
+            project<T, T>(g, flow[0].data(), correction[ci].data(), flow[1].data());
+            lastCorrection = ci;
+            lastCorrectionShared = false;
         } else if (mode == FIREX_PRESSURE_WARM_F32) {  // branch A (FireXEngine.ts:2248-2273)
             for (int i = 0; i < P; ++i) {
                 jacobi_sweep<T, T>(g, pressure[pressureIndex].data(), divergence.data(), pressure[1 - pressureIndex].data());
@@ -1187,7 +1213,8 @@ struct Sim : SimBase {
             case FIREX_FIELD_FLOW: return copy_out_vec4<float>(flow[0], out, bytes);
             case FIREX_FIELD_SPECIES: return copy_out_vec4<float>(species[speciesIndex], out, bytes);
             case FIREX_FIELD_PRESSURE:
-                if (mode == FIREX_PRESSURE_F16) return copy_out_half(pressure16[pressureIndex], out, bytes);
+                if (mode == FIREX_PRESSURE_F16 || mode == FXO_PRESSURE_F16P_F32C)
+                    return copy_out_half(pressure16[pressureIndex], out, bytes);
                 return copy_out_scalar(pressure[pressureIndex], out, bytes);
             case FIREX_FIELD_DIVERGENCE: return copy_out_scalar(divergence, out, bytes);
             case FIREX_FIELD_REACTION: return copy_out_scalar(reaction, out, bytes);
@@ -1297,7 +1324,8 @@ struct Sim : SimBase {
             case FIREX_FIELD_FLOW: return write_vec4(flow[0], in, bytes);
             case FIREX_FIELD_SPECIES: return write_vec4(species[speciesIndex], in, bytes);
             case FIREX_FIELD_PRESSURE:
-                if (mode == FIREX_PRESSURE_F16) return write_half(pressure16[pressureIndex], in, bytes);
+                if (mode == FIREX_PRESSURE_F16 || mode == FXO_PRESSURE_F16P_F32C)
+                    return write_half(pressure16[pressureIndex], in, bytes);
                 return write_scalar(pressure[pressureIndex], in, bytes);
             case FIREX_FIELD_DIVERGENCE: return write_scalar(divergence, in, bytes);
             case FIREX_FIELD_REACTION: return write_scalar(reaction, in, bytes);

@@ -31,6 +31,11 @@ def test_reference_arm_prints_one_contract_line():
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["e2e"]["value"] == line["value"]
+    # both arms describe the same workload with the same warm-up
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert line["config"] == json.loads(json.dumps(bench.config()))
+    assert line["warmup"] == 1
 
 
 def test_reference_arm_other_ranks_exit_quietly():

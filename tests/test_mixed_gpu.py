@@ -48,13 +48,23 @@ def rel_div(test, ref64, pre_l2):
 
 
 def field_errors(test, ref64):
+    """Max-abs error per field against the FP64 step, and the same relative to the FP64
+    field's largest magnitude (max-rel)."""
     f, g = test.read("flow"), ref64.read("flow")
-    return {"flow_uvw": max_abs(f[..., :3], g[..., :3]), "flow_T": max_abs(f[..., 3], g[..., 3]),
-            "species": max_abs(test.read("species"), ref64.read("species")),
-            "pressure": max_abs(test.read("pressure"), ref64.read("pressure"))}
+    pairs = {"flow_uvw": (f[..., :3], g[..., :3]), "flow_T": (f[..., 3], g[..., 3]),
+             "species": (test.read("species"), ref64.read("species")),
+             "pressure": (test.read("pressure"), ref64.read("pressure")),
+             "correction": (test.read("correction"), ref64.read("correction"))}
+    out = {}
+    for k, (a, b) in pairs.items():
+        e = max_abs(a, b)
+        out[k] = e
+        out[k + "_rel"] = e / max(float(np.abs(b).max()), 1e-30)
+    return out
 
 
-@pytest.mark.parametrize("dims,P,R,warm", [((64, 96, 64), 40, 40, 8), ((96, 144, 96), 96, 96, 4)])
+@pytest.mark.parametrize("dims,P,R,warm", [((64, 96, 64), 40, 40, 8), ((96, 144, 96), 96, 96, 4),
+                                           ((160, 240, 160), 96, 96, 2)])
 def test_mixed_step_divergence_vs_fp64(dims, P, R, warm):
     """One step from the FP64 oracle's state after `warm` steps, in FP32 and mixed form."""
     opts = sphere_options(dims, P=P, R=R)
@@ -71,13 +81,20 @@ def test_mixed_step_divergence_vs_fp64(dims, P, R, warm):
     for g in (g32, gmx, g16):
         g.step(1, DT)
     e32, emx, e16 = rel_div(g32, o64, pre), rel_div(gmx, o64, pre), rel_div(g16, o64, pre)
+    fmx, f32 = field_errors(gmx, o64), field_errors(g32, o64)
     report(f"mixed_step_{dims[0]}x{dims[1]}x{dims[2]}", rel_div_f32=e32, rel_div_mixed=emx, rel_div_f16_pressure=e16,
            post_over_pre_fp64=o64.divergence_norm()[0] / pre,
-           **{f"mixed_{k}": v for k, v in field_errors(gmx, o64).items()},
-           **{f"f32_{k}": v for k, v in field_errors(g32, o64).items()})
+           **{f"mixed_{k}": v for k, v in fmx.items()}, **{f"f32_{k}": v for k, v in f32.items()})
     assert e32 <= REL_DIV_F32, e32
     assert emx <= REL_DIV_MIXED, emx
     assert e16 <= REL_DIV_F16_PRESSURE, e16
+    # FP16 species: the FP16 input (the FP64 state rounded on write) carried through one
+    # step plus the rounding of the stored result, each within an FP16 ULP of the largest
+    # species value (2^-10 relative); the FP32 fields move only by what the species change
+    # in the source terms
+    assert fmx["species_rel"] <= 2.0 ** -10 + f32["species_rel"], (fmx, f32)
+    for k in ("flow_uvw_rel", "flow_T_rel", "pressure_rel", "correction_rel"):
+        assert fmx[k] <= 1e-3, (k, fmx, f32)
 
 
 def test_mixed_trajectory_divergence_norm_vs_fp64():

@@ -89,3 +89,27 @@ def test_noalloc_rejects_beyond_scratch_and_misaligned():
     # a grid without interior cells launches nothing and reports zeros
     rc, got = _noalloc(lib, flow.data_ptr(), (2, 2, 4), [1.0, 1.0, 1.0])
     assert rc == A.OK and got == (0.0, 0.0, 0.0)
+
+
+def test_noalloc_rejects_short_buffers_and_host_memory():
+    """Dims that need more flow records than the caller's allocation holds, and a host
+    pointer, are refused before any launch; the calling thread's current device is left as
+    it was."""
+    import torch
+
+    lib = load_library()
+    dev_before = torch.cuda.current_device()
+    small = torch.zeros(64, dtype=torch.float32, device="cuda")  # inside a 2 MiB cached segment
+    rc, _ = _noalloc(lib, small.data_ptr(), (256, 256, 64), [1.0, 1.0, 1.0])  # 64 MiB of records
+    assert rc == A.ERR_BAD_ARG
+    assert b"allocation" in lib.firex_last_error(None)
+    host = np.zeros(8 * 8 * 8 * 4, np.float32)
+    ptr = host.ctypes.data + (-host.ctypes.data) % 16
+    rc, _ = _noalloc(lib, ptr, (4, 4, 4), [1.0, 1.0, 1.0])
+    assert rc == A.ERR_BAD_ARG
+    assert torch.cuda.current_device() == dev_before
+    # a valid call afterwards still works, and leaves the current device alone
+    flow = torch.zeros(6 * 6 * 6 * 4, dtype=torch.float32, device="cuda")
+    rc, got = _noalloc(lib, flow.data_ptr(), (6, 6, 6), [1.0, 1.0, 1.0])
+    assert rc == A.OK and got == (0.0, 0.0, 64.0)
+    assert torch.cuda.current_device() == dev_before
