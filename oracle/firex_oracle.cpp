@@ -6,9 +6,14 @@
 //
 // Parity status: the reference is WGSL run by WebGPU from TypeScript; neither a WebGPU
 // implementation nor a JS runtime exists here, and the reference's own tests hold no
-// numeric golden vectors for this path. The numeric level is therefore UNPINNED: this
-// restatement follows the reference source line by line (citations below) and the
-// contracts its tests assert are re-asserted by tests/test_oracle_contracts.py.
+// numeric golden vectors for this path. The step is PINNED instead to the reference's own
+// kernels executed on the CPU: tests/golden/wgsl_eval.py evaluates the WGSL text of
+// shaders.ts:1-512 and pressureShaders.ts:1-161 in the dispatch order of
+// FireXEngine.ts:2115-2276, and tests/test_reference_golden.py requires this restatement to
+// reproduce those fixtures bit for bit (all three pressure branches, reset and developed
+// states, dt = 0, 1/60, 1/30, a non-default parameter set). The contracts the reference's
+// tests assert are re-asserted by tests/test_oracle_contracts.py. The droplet passes are
+// pinned against a numpy restatement only (tests/test_sph.py).
 //
 // Arithmetic conventions (shared with the CUDA kernels, which must match them):
 //   * every WGSL expression is evaluated left to right in the precision T with no fused
