@@ -187,6 +187,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_write_particles": (C.c_int, [vp, vp, C.c_size_t]),
         "firex_divergence_norm_noalloc": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_float), vp,
                                                     C.POINTER(C.c_double)]),
+        "firex_set_wait_limit": (C.c_int, [vp, C.c_uint32]),
+        "firex_test_hold_face": (C.c_int, [vp, C.c_int32, C.c_int32]),
         "firex_get_state": (C.c_int, [vp, C.POINTER(State)]),
         "firex_set_state": (C.c_int, [vp, C.POINTER(State)]),
         "firex_get_uniforms": (C.c_int, [vp, C.c_double, C.POINTER(C.c_float)]),
@@ -224,7 +226,7 @@ HEADER_SYMBOLS = [
     "firex_last_error", "firex_set_parameter", "firex_get_parameter", "firex_reset", "firex_step",
     "firex_sync", "firex_read_field", "firex_read_field_async", "firex_write_field", "firex_divergence_norm",
     "firex_set_render_packing", "firex_render_volumes", "firex_read_particles", "firex_write_particles",
-    "firex_divergence_norm_noalloc", "firex_get_state",
+    "firex_divergence_norm_noalloc", "firex_set_wait_limit", "firex_test_hold_face", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_preflight", "firex_stream", "firex_set_profiling", "firex_pass_times",
     "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_batch_create", "firex_batch_destroy",

@@ -5,8 +5,8 @@ Every Jacobi kernel of the library computes each sweep with the same FP32 operat
 the same order (the GPU tests hold them bit-identical), so the steps taken while tuning are
 ordinary steps of the run: the trajectory is the same whichever candidate ran them. The
 candidates are the resident kernel in each box variant that fits, the single-sweep kernels
-(unblocked, and z-marching with 8, 16 or 32 planes per CTA) and the fused kernels (two
-sweeps per pass with 16-, 32- or 64-plane chunks, four sweeps per launch). The winner is
+(unblocked, and z-marching with 8, 16 or 32 planes per CTA) and the two-sweep pass with 16-,
+32- or 64-plane chunks. The winner is
 applied with set_jacobi and remembered per workload signature (grid sizes, sweep counts,
 precision, pressure branch), optionally in a JSON file so that a later process starts tuned.
 """
@@ -38,7 +38,6 @@ def default_candidates() -> list:
     out += [Candidate("unblocked")]
     out += [Candidate("zmarch", 0, zc) for zc in (8, 16, 32)]
     out += [Candidate("fused", 2, zc) for zc in (16, 32, 64)]
-    out += [Candidate("fused", 4, zc) for zc in (8, 16)]
     return out
 
 

@@ -199,7 +199,7 @@ struct FxResBox {
 };
 // CELL: 32 x 4 x 2 cells, one thread per cell (simulate).
 // ROW4: 256 groups of 4 consecutive x cells in memory order (stencils).
-// COL : column tiles of the temporally blocked Jacobi (see fx_jacobi_tb.cuh).
+// COL : tiles x z chunks of the two-sweep Jacobi pass (see fx_jacobi_zm2.cuh).
 // ZM  : z-marching tiles of the single-sweep Jacobi (see fx_jacobi_zm.cuh).
 // TAB : 256 entries of the per-step tables of simulate.
 #define FX_CELL_BX 32

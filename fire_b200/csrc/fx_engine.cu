@@ -24,7 +24,6 @@
 #include "../../include/firex.h"
 #include "fx_internal.h"
 #include "fx_jacobi_res.cuh"
-#include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
 #include "fx_jacobi_zm2.cuh"
 
@@ -183,8 +182,7 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     fx_launch_simulate(st, pl.storage, B, pl.bricks[FX_SHAPE_CELL]);
     fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 0);
     enqueue_jacobi_phase(st, pl, B, 0);
-    fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 0);
-    fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 1);
+    fx_launch_project_div(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4]);
     enqueue_jacobi_phase(st, pl, B, 1);
     fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 1);
     fx_launch_step_end(st, B);
@@ -651,7 +649,7 @@ struct firex_batch {
             acc[FX_SHAPE_TAB] += (fx_tab_layout(s->X, s->Y, s->Z).total + 255) / 256;
             acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z);
             acc[FX_SHAPE_ROW4] += (int)bricks_row4(s->X, s->Y, s->Z);
-            acc[FX_SHAPE_COL] += k == 2 ? fx_zm2_bricks(s->X, s->Y, s->Z, zc) : (k > 1 ? fx_tb_bricks(s->X, s->Y, s->Z, k, zc) : 0);
+            acc[FX_SHAPE_COL] += k == 2 ? fx_zm2_bricks(s->X, s->Y, s->Z, zc) : 0;
             acc[FX_SHAPE_ZM] += fx_zm_bricks(s->X, s->Y, s->Z, zmZc);
         }
         for (int j = 0; j < FX_NSHAPES; ++j) {
@@ -784,10 +782,8 @@ struct firex_batch {
         mark(FIREX_PASS_DIVERGENCE, 1);
         enqueue_jacobi_phase(stream, pl, d, 0);
         mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 0));
-        fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 0);
+        fx_launch_project_div(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4]);
         mark(FIREX_PASS_PROJECT, 1);
-        fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 1);
-        mark(FIREX_PASS_DIVERGENCE, 1);
         enqueue_jacobi_phase(stream, pl, d, 1);
         mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 1));
         fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 1);
@@ -858,7 +854,7 @@ struct firex_batch {
             if (!profiling) {
                 pendingLaunches[FIREX_PASS_OTHER] += pl.pack ? 4 : 3;
                 pendingLaunches[FIREX_PASS_SIMULATE] += 1;
-                pendingLaunches[FIREX_PASS_DIVERGENCE] += 2;
+                pendingLaunches[FIREX_PASS_DIVERGENCE] += 1;
                 pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
                 pendingLaunches[FIREX_PASS_PROJECT] += 2;
                 pendingLaunches[FIREX_PASS_PARTICLES] += sph_launches(pl);
@@ -1157,7 +1153,8 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         (opt->emitter_mode != FIREX_EMITTER_BURNER && opt->emitter_mode != FIREX_EMITTER_SPHERES) ||
         opt->pressure_mode < FIREX_PRESSURE_AUTO || opt->pressure_mode > FIREX_PRESSURE_COLD_F32 ||
         (opt->precision != FIREX_PRECISION_F32 && opt->precision != FIREX_PRECISION_MIXED) ||
-        !(opt->velocity_noise >= 0) || !(opt->emission_jitter >= 0)) {
+        !(opt->velocity_noise >= 0) || !(opt->emission_jitter >= 0) || opt->jacobi_block < 0 ||
+        opt->jacobi_block > 2) {
         g_create_error = "invalid options";
         return FIREX_ERR_BAD_ARG;
     }
@@ -1314,6 +1311,29 @@ int firex_sync(firex_sim* s) {
     if (e != cudaSuccess) return s->cuda_fail(e, "sync");
     s->copyPending = false;
     return s->check_device_waits();
+}
+
+// Writes sync words [first, first + n) of the simulation in stream order (the kernels read
+// them at run time, so captured step graphs see the new values).
+static int write_sync_words(firex_sim* s, int first, const unsigned* v, int n) {
+    if (s->poisoned) return s->fail(FIREX_ERR_STATE, "handle is poisoned by an earlier error");
+    DeviceGuard dg(s->device);
+    cudaError_t e = cudaMemcpyAsync(s->h.sync + first, v, n * sizeof(unsigned), cudaMemcpyHostToDevice, s->stream());
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream());
+    if (e != cudaSuccess) return s->cuda_fail(e, "sync words");
+    return FIREX_OK;
+}
+
+int firex_set_wait_limit(firex_sim* s, uint32_t polls) {
+    if (!s) return FIREX_ERR_BAD_ARG;
+    return write_sync_words(s, FX_SYNC_SPIN, &polls, 1);
+}
+
+int firex_test_hold_face(firex_sim* s, int32_t box, int32_t sweep) {
+    if (!s) return FIREX_ERR_BAD_ARG;
+    if (box >= FX_RES_MAX_CTAS || (box >= 0 && sweep < 0)) return s->fail(FIREX_ERR_BAD_ARG, "box or sweep out of range");
+    const unsigned v[2] = {box >= 0 ? (unsigned)box + 1u : 0u, box >= 0 ? (unsigned)sweep : 0u};
+    return write_sync_words(s, FX_SYNC_HOLD_BOX, v, 2);
 }
 
 // Device buffer and element size backing a field in the current parity, for direct copies.
@@ -1574,7 +1594,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
     out->launches_per_step =
-        8 + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+        7 + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     out->jacobi_variant = p.res ? p.resVariant : -1;
@@ -1584,7 +1604,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
 static bool jacobi_args_ok(int32_t kernel, int32_t block, int32_t zchunk) {
     if (kernel < FIREX_JACOBI_AUTO || kernel > FIREX_JACOBI_RESIDENT || zchunk < 0 || zchunk > 4096) return false;
     if (kernel == FIREX_JACOBI_RESIDENT) return block >= 0 && block <= 4;
-    return kernel != FIREX_JACOBI_FUSED || block == 2 || block == 3 || block == 4 || block == 6;
+    return kernel != FIREX_JACOBI_FUSED || block == 2;
 }
 // the block argument kept per kernel: sweeps per launch (FUSED), variant + 1 (RESIDENT)
 static int jacobi_block_kept(int32_t kernel, int32_t block) {

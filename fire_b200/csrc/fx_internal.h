@@ -24,6 +24,9 @@ void fx_launch_jacobi_zm(cudaStream_t s, bool half, const FxBatchDev* B, int bri
 enum { FX_TB_F32 = 0, FX_TB_F16_ROUND = 1, FX_TB_F16 = 2 };
 bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc);
 void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase);
+// The primary projection (phase 0) and the divergence of its result (the residual solve's
+// right-hand side) in one pass.
+void fx_launch_project_div(cudaStream_t s, bool half, const FxBatchDev* B, int bricks);
 // Every sweep of a phase in one cooperative launch of `ctas` CTAs with `smem` bytes of
 // dynamic shared memory (fx_jacobi_res.cuh; variant 0 column, 1 faces-first, 2 faces-first
 // for small boxes);

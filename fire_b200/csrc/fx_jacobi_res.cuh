@@ -25,8 +25,9 @@
 // primary and residual solves, so the other buffer is observable there).
 //
 // A cooperative launch guarantees that every CTA is resident, so every neighbour flag
-// arrives; the waits are still bounded (FX_RES_SPIN_LIMIT polls): on expiry the CTA
-// sets the simulation's error word and returns, and the host reports a timeout.
+// arrives; the waits are still bounded (FX_RES_SPIN_LIMIT polls, or the simulation's own
+// limit): on expiry the CTA sets the simulation's error word and returns, its neighbours'
+// waits for it then expire in turn, every CTA returns, and the host reports a timeout.
 #pragma once
 
 #include "fx_step_math.cuh"
@@ -43,6 +44,14 @@
 #define FX_RES_MAX_CTAS 1024          // boxes per simulation and phase (flag slots)
 #define FX_RES_FLAGS 16               // offset of the flag slots in FxSimDev::sync
 #define FX_RES_SYNC_WORDS (FX_RES_FLAGS + 2 * FX_RES_MAX_CTAS)
+// Words of FxSimDev::sync after the error word [2], set from the host (firex_set_wait_limit,
+// firex_test_hold_face) and zero by default:
+//   [3] polls of a neighbour's flag before a wait gives up (0: FX_RES_SPIN_LIMIT);
+//   [4] box + 1 that does not publish its faces of sweep [5] (0: every box publishes) — a
+//       flag that nothing sets, so the neighbours' bounded waits expire (test of the error path).
+#define FX_SYNC_SPIN 3
+#define FX_SYNC_HOLD_BOX 4
+#define FX_SYNC_HOLD_SWEEP 5
 
 // Shared-memory bytes of a box: pressure with halo rows + divergence.
 __host__ __device__ inline long long fx_res_smem_bytes(int X, int by, int bz) {
@@ -74,6 +83,22 @@ FXD void fx_st_release_u32(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
 }
 
+// The sync words of the simulation whose error word is `err`.
+FXD const unsigned* fx_res_sync(const unsigned* err) { return err - 2; }
+
+// Polls before a wait gives up.
+FXD unsigned fx_res_spin_limit(const unsigned* err) {
+    const unsigned v = fx_res_sync(err)[FX_SYNC_SPIN];
+    return v ? v : FX_RES_SPIN_LIMIT;
+}
+
+// Publishes box `me`'s faces of sweep s (flag = s + 1, release), unless the host holds them back.
+FXD void fx_res_publish(unsigned* flags, int me, unsigned s, const unsigned* err) {
+    const unsigned* sync = fx_res_sync(err);
+    if (sync[FX_SYNC_HOLD_BOX] == (unsigned)me + 1 && sync[FX_SYNC_HOLD_SWEEP] == s) return;
+    fx_st_release_u32(flags + me, s + 1);
+}
+
 // Waits until each neighbour box has published sweep s (flag >= s + 1: acquire loads, one
 // thread per neighbour, each wait bounded), then synchronises the CTA. False when a wait
 // expired (the error word is then set).
@@ -81,9 +106,10 @@ FXD bool fx_res_wait(const unsigned* flags, const int nb[4], unsigned s, unsigne
     if (threadIdx.x == 0) *flag = 1;
     __syncthreads();
     if (threadIdx.x < 4 && nb[threadIdx.x] >= 0) {
+        const unsigned limit = fx_res_spin_limit(err);
         unsigned spins = 0;
         while (fx_ld_acquire_u32(flags + nb[threadIdx.x]) < s + 1) {
-            if (++spins > FX_RES_SPIN_LIMIT) {
+            if (++spins > limit) {
                 atomicExch(err, 1u);
                 *flag = 0;
                 break;
@@ -103,13 +129,14 @@ FXD bool fx_res_exchange(unsigned* flags, int me, const int nb[4], unsigned s, u
     __syncthreads();
     if (threadIdx.x == 0) {
         *flag = 1;
-        fx_st_release_u32(flags + me, s + 1);
+        fx_res_publish(flags, me, s, err);
     }
     __syncthreads();
     if (threadIdx.x < 4 && nb[threadIdx.x] >= 0) {
+        const unsigned limit = fx_res_spin_limit(err);
         unsigned spins = 0;
         while (fx_ld_acquire_u32(flags + nb[threadIdx.x]) < s + 1) {
-            if (++spins > FX_RES_SPIN_LIMIT) {
+            if (++spins > limit) {
                 atomicExch(err, 1u);
                 *flag = 0;
                 break;
@@ -437,7 +464,7 @@ FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phas
         }
         if (!last) {
             __syncthreads();  // every face store of this CTA precedes the flag (release is cumulative)
-            if (t == 0) fx_st_release_u32(cx.flags + b, (unsigned)s + 1);
+            if (t == 0) fx_res_publish(cx.flags, b, (unsigned)s, cx.err);
         }
         float4 nv[MAXI];
 #pragma unroll
@@ -579,7 +606,7 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         }
         if (!last) {
             __syncthreads();  // every face store of this CTA precedes the flag (release is cumulative)
-            if (t == 0) fx_st_release_u32(cx.flags + b, (unsigned)s + 1);
+            if (t == 0) fx_res_publish(cx.flags, b, (unsigned)s, cx.err);
         }
         float4 nv[FX_RES_MAXZ];
         {
@@ -616,9 +643,10 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         // the neighbours' faces of this sweep: the waiting threads spin before the barrier
         // that also ends every read of the old values
         if (!last && t < 4 && cx.nb[t] >= 0) {
+            const unsigned limit = fx_res_spin_limit(cx.err);
             unsigned spins = 0;
             while (fx_ld_acquire_u32(cx.flags + cx.nb[t]) < (unsigned)s + 1) {
-                if (++spins > FX_RES_SPIN_LIMIT) {
+                if (++spins > limit) {
                     atomicExch(cx.err, 1u);
                     s_flag = 0;
                     break;

@@ -16,7 +16,6 @@
 #include "fx_internal.h"
 #include "fx_jacobi_res.cuh"
 #include "fx_sph.cuh"
-#include "fx_jacobi_tb.cuh"
 #include "fx_jacobi_zm.cuh"
 #include "fx_jacobi_zm2.cuh"
 #include "fx_step_math.cuh"
@@ -330,6 +329,112 @@ __global__ void __launch_bounds__(256, 8) fxk_project(const FxBatchDev* __restri
     });
 }
 
+// ---- primary projection fused with the residual's divergence -----------------------------
+// projectVelocity with the primary pressure (phase 0 above) followed by computeDivergence of
+// its result (shaders.ts:344-364; FireXEngine.ts:2256-2257 runs them as two dispatches) in one
+// pass: the projected flow is written and its backward divergence stored as the residual
+// solve's right-hand side, without reading the projected flow back. The backward neighbours'
+// projected components are recomputed with the projection's own operations, so every value
+// is bit-identical to the two separate passes:
+//   u of the cell before:  the lane before (shuffle), lane 31 of the previous group, or for a
+//                          warp's first cell the projection of x - 1 recomputed;
+//   v of the row below:    the projection of (x, y - 1, z), never a top-row cell;
+//   w of the plane behind: the projection of (x, y, z - 1), from the row below when y is the
+//                          top row (the top row copies the projected row below).
+// The extra loads (one component of the flow and one pressure value per neighbour) hit
+// L1/L2: the rows and planes behind were read by the warps and CTAs before.
+template <typename PT>
+struct ProjSrc {
+    const float4* __restrict__ flowIn;
+    const void* p;
+    bool zeroP;
+    int X, Y, Z, XY;
+    float3 m;
+    FXD float pr(int i) const { return zeroP ? 0.0f : PStore<PT>::ld(p, i); }
+    // u of cell c = (x, y, z), x in [1, X - 2] (the walls force u = 0 and need no load)
+    FXD float u(int c, int x, int y) const {
+        if (x == 0 || x == X - 1) return 0.0f;
+        const int cs = (y == Y - 1) ? c - X : c;
+        const float pc = pr(cs);
+        const float px = pr(cs + 1);
+        return __ldg(&flowIn[cs].x) - (px - pc) * m.x;
+    }
+    // v of cell c = (x, y, z) with y <= Y - 2
+    FXD float v(int c, int y) const {
+        if (y == 0) return 0.0f;
+        const float pc = pr(c);
+        const float pt = pr(c + X);
+        return __ldg(&flowIn[c].y) - (pt - pc) * m.y;
+    }
+    // w of cell c = (x, y, z) with z <= Z - 2
+    FXD float w(int c, int y, int z) const {
+        if (z == 0) return 0.0f;
+        const int cs = (y == Y - 1) ? c - X : c;
+        const float pc = pr(cs);
+        const float pf = pr(cs + XY);
+        return __ldg(&flowIn[cs].z) - (pf - pc) * m.z;
+    }
+};
+
+template <typename PT>
+__global__ void __launch_bounds__(256, 4) fxk_project_div(const FxBatchDev* __restrict__ B) {
+    fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
+        const Lane4 r = fx_lane4(S, b);
+        if (r.n <= 0) return;  // warp-uniform
+        const int lane = threadIdx.x & 31;
+        const int base = (S.mode == FIREX_PRESSURE_COLD_F32) ? 0 : S.pi;
+        ProjSrc<PT> src{reinterpret_cast<const float4*>(S.flow[S.fi ^ 1]), S.p[(base + S.P) & 1],
+                        S.mode == FIREX_PRESSURE_COLD_F32 && S.P == 0, S.X, S.Y, S.Z, S.X * S.Y, fx_metric(S.prm.u)};
+        float4* __restrict__ flowOut = reinterpret_cast<float4*>(S.flow[S.fi]);
+        const int X = S.X, XY = S.X * S.Y;
+        int xs[4], ys[4], zs[4];
+        fx_lane4_coords(S, r, xs, ys, zs);
+        float4 o[4];
+        float vb[4], wk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            o[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            vb[i] = wk[i] = 0.0f;
+            if (lane + 32 * i < r.n) {
+                const int c = r.c0 + 32 * i;
+                const int cs = (ys[i] == S.Y - 1) ? c - X : c;  // top row: the projected row below
+                const float4 f = __ldg(src.flowIn + c);
+                const float4 s = (cs == c) ? f : __ldg(src.flowIn + cs);
+                float pc = 0.0f, px = 0.0f, pt = 0.0f, pf = 0.0f;
+                if (!src.zeroP) {
+                    pc = PStore<PT>::ld(src.p, cs);
+                    px = xs[i] + 1 < X ? PStore<PT>::ld(src.p, cs + 1) : pc;
+                    pt = PStore<PT>::ld(src.p, cs + X);
+                    pf = zs[i] < S.Z - 1 ? PStore<PT>::ld(src.p, cs + XY) : pc;
+                }
+                const float gx = (px - pc) * src.m.x;
+                const float gy = (pt - pc) * src.m.y;
+                const float gz = (pf - pc) * src.m.z;
+                float4 q = make_float4(s.x - gx, s.y - gy, s.z - gz, f.w);
+                if (xs[i] == 0 || xs[i] == X - 1) q.x = 0.0f;
+                if (zs[i] == 0 || zs[i] == S.Z - 1) q.z = 0.0f;
+                if (ys[i] == 0) q.y = 0.0f;
+                if (ys[i] == S.Y - 1) q.y = fx_max(0.0f, q.y);
+                flowOut[c] = q;
+                o[i] = q;
+                vb[i] = ys[i] > 0 ? src.v(c - X, ys[i] - 1) : q.y;
+                wk[i] = zs[i] > 0 ? src.w(c - XY, ys[i], zs[i] - 1) : q.z;
+            }
+        }
+        // u of the cell before lane 0's first cell (another warp's or brick's cell)
+        float prevU = (lane == 0 && r.n > 0 && xs[0] > 0) ? src.u(r.c0 - 1, xs[0] - 1, ys[0]) : 0.0f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float fromLeft = __shfl_up_sync(0xffffffffu, o[i].x, 1);
+            const float ul = xs[i] == 0 ? o[i].x : (lane > 0 ? fromLeft : prevU);
+            prevU = __shfl_sync(0xffffffffu, o[i].x, 31);
+            if (lane + 32 * i < r.n)
+                S.div[r.c0 + 32 * i] =
+                    (o[i].x - ul) * src.m.x + (o[i].y - vb[i]) * src.m.y + (o[i].z - wk[i]) * src.m.z;
+        }
+    });
+}
+
 // ---- one Jacobi sweep by z-marching tiles (fx_jacobi_zm.cuh) ---------------------------------
 template <typename PT>
 __global__ void __launch_bounds__(FX_ZM_THREADS, 3) fxk_jacobi_zm(const FxBatchDev* __restrict__ B, int phase, int launch,
@@ -356,23 +461,6 @@ __global__ void __launch_bounds__(FX_ZM_THREADS, 3) fxk_jacobi_zm(const FxBatchD
             else if (TX == 64) fx_zm_tile<PT, false, 64>(&S, pin, pout, x0, y0, z0, z1, sm);
             else fx_zm_tile<PT, false, 32>(&S, pin, pout, x0, y0, z0, z1, sm);
         }
-    });
-}
-
-// ---- K fused Jacobi sweeps per launch (fx_jacobi_tb.cuh) ------------------------------------
-template <int K, typename PT, bool ROUND>
-__global__ void __launch_bounds__(FX_TB_THREADS, 1) fxk_jacobi_tb(const FxBatchDev* __restrict__ B, int phase, int launch, int zc) {
-    extern __shared__ __align__(16) float fx_tb_dyn[];
-    auto sm = reinterpret_cast<float(*)[FX_TB_RY][FX_TB_RX]>(fx_tb_dyn);
-    auto dsm = reinterpret_cast<float(*)[FX_TB_RY][FX_TB_RX]>(fx_tb_dyn + K * FX_TB_RY * FX_TB_RX);
-    fx_for_bricks<FX_SHAPE_COL>(B, [&](const FxSimDev& S, int b) {
-        constexpr int TX = FxTbShape<K>::TX, TY = FxTbShape<K>::TY;
-        const int ntx = (S.X + TX - 1) / TX, nty = (S.Y + TY - 1) / TY;
-        const int tx = b % ntx, ty = (b / ntx) % nty, zci = b / (ntx * nty);
-        const int z0 = zci * zc, z1 = min(S.Z, z0 + zc);
-        const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
-        fx_tb_column<K, PT, ROUND>(S, bufs.pin, bufs.pout, bufs.zeroIn, tx, ty, z0, z1, sm, dsm);
-        __syncthreads();  // the planes are reused by the next brick
     });
 }
 
@@ -738,28 +826,6 @@ void fx_launch_jacobi_zm(cudaStream_t s, bool half, const FxBatchDev* B, int bri
     else launch_zm<float>(s, B, bricks, phase, launch, sweep, zc);
 }
 
-template <int K, typename PT, bool ROUND>
-static int tb_grid() {
-    constexpr int smem = fx_tb_smem_bytes(K);
-    cudaFuncSetAttribute((const void*)fxk_jacobi_tb<K, PT, ROUND>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fxk_jacobi_tb<K, PT, ROUND>, FX_TB_THREADS, smem);
-    return (per_sm > 0 ? per_sm : 1) * num_sms();
-}
-
-template <int K, typename PT, bool ROUND>
-static void launch_tb(cudaStream_t s, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
-    static int g = tb_grid<K, PT, ROUND>();
-    fxk_jacobi_tb<K, PT, ROUND><<<bricks < g ? bricks : g, FX_TB_THREADS, fx_tb_smem_bytes(K), s>>>(B, phase, launch, zc);
-}
-
-template <int K>
-static void launch_tb_k(cudaStream_t s, int pmode, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
-    if (pmode == FX_TB_F32) launch_tb<K, float, false>(s, B, bricks, phase, launch, zc);
-    else if (pmode == FX_TB_F16_ROUND) launch_tb<K, __half, true>(s, B, bricks, phase, launch, zc);
-    else launch_tb<K, __half, false>(s, B, bricks, phase, launch, zc);
-}
-
 template <typename PT, bool ROUND>
 static void launch_zm2(cudaStream_t s, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
     static int g = [] {
@@ -780,9 +846,6 @@ bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, 
             else if (pmode == FX_TB_F16_ROUND) launch_zm2<__half, true>(s, B, bricks, phase, launch, zc);
             else launch_zm2<__half, false>(s, B, bricks, phase, launch, zc);
             return true;
-        case 3: launch_tb_k<3>(s, pmode, B, bricks, phase, launch, zc); return true;
-        case 4: launch_tb_k<4>(s, pmode, B, bricks, phase, launch, zc); return true;
-        case 6: launch_tb_k<6>(s, pmode, B, bricks, phase, launch, zc); return true;
     }
     return false;
 }
@@ -845,6 +908,16 @@ void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int brick
     } else {
         static int g = persistent_grid((const void*)fxk_project<float>, 256, 1 << 30);
         fxk_project<float><<<row4_grid(g, bricks), 256, 0, s>>>(B, phase);
+    }
+}
+
+void fx_launch_project_div(cudaStream_t s, bool half, const FxBatchDev* B, int bricks) {
+    if (half) {
+        static int g = persistent_grid((const void*)fxk_project_div<__half>, 256, 1 << 30);
+        fxk_project_div<__half><<<row4_grid(g, bricks), 256, 0, s>>>(B);
+    } else {
+        static int g = persistent_grid((const void*)fxk_project_div<float>, 256, 1 << 30);
+        fxk_project_div<float><<<row4_grid(g, bricks), 256, 0, s>>>(B);
     }
 }
 

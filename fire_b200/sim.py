@@ -278,6 +278,15 @@ class FireXSim(_Handle):
     def stream(self) -> int:
         return self._lib.firex_stream(self._h) or 0
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls before a bounded device wait gives up (0: the library's limit)."""
+        self._check(self._lib.firex_set_wait_limit(self._h, int(polls)))
+
+    def test_hold_face(self, box: int, sweep: int) -> None:
+        """Test hook: box `box` of the resident Jacobi withholds its faces of sweep `sweep`
+        (box < 0 clears it), so that its neighbours' bounded waits expire."""
+        self._check(self._lib.firex_test_hold_face(self._h, int(box), int(sweep)))
+
     def set_jacobi(self, kernel, block: int = 0, zchunk: int = 0) -> None:
         """Jacobi kernel: 'auto', 'unblocked', 'zmarch', 'fused' (with `block` sweeps per
         launch) or 'resident' (`block` = box variant + 1, 0 = planner's choice), and z planes

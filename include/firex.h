@@ -84,7 +84,7 @@ typedef struct firex_options {
     float velocity_noise;          /* initial velocity: uniform in [-a, a] per component */
     float emission_jitter;         /* per-step emission factor uniform in [1-a, 1+a] */
     int32_t cinematic;             /* mixing.z; offline tiers force 1 (FireXEngine.ts:2097,2819) */
-    int32_t jacobi_block;          /* > 1: fuse this many Jacobi sweeps per launch (see firex_set_jacobi) */
+    int32_t jacobi_block;          /* 2: two Jacobi sweeps per launch (FUSED, see firex_set_jacobi); 0/1: AUTO */
     uint64_t memory_budget_bytes;  /* 0 = no budget; else create fails with FIREX_ERR_BUDGET */
     int32_t jacobi_zchunk;         /* z planes per CTA of a fused Jacobi launch; 0 = auto */
     int32_t particle_count;        /* SPH droplets (FIREX_QUALITY particleCount, FireXEngine.ts:187-277);
@@ -227,6 +227,18 @@ int firex_divergence_norm(firex_sim* sim, double out[3]);
 int firex_divergence_norm_noalloc(const void* flow, const int32_t dims[3], const float metric[3], void* stream,
                                   double out[3]);
 
+/* Bounded device waits. The resident Jacobi's CTAs wait on their neighbours' flags; a wait
+ * gives up after `polls` polls (0: the library's limit, well over a second), sets the
+ * simulation's error word and returns, and the next firex_sync / firex_batch_sync answers
+ * FIREX_ERR_TIMEOUT and poisons the handle (the reference's device-lost state,
+ * FireXEngine.ts:538-542,2887-2897: later calls fail with FIREX_ERR_STATE). */
+int firex_set_wait_limit(firex_sim* sim, uint32_t polls);
+
+/* Test hook for the error path above (no reference counterpart): from the next step on, box
+ * `box` of the resident Jacobi does not publish its faces of sweep `sweep` (in either phase),
+ * a flag that nothing sets, so its neighbours' bounded waits expire. box < 0 clears it. */
+int firex_test_hold_face(firex_sim* sim, int32_t box, int32_t sweep);
+
 /* Counters that decide ping-pong parity and time (FireXEngine.ts:396-409). */
 int firex_get_state(const firex_sim* sim, firex_state* st);
 int firex_set_state(firex_sim* sim, const firex_state* st);
@@ -313,13 +325,13 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
  *   UNBLOCKED — one thread per 4 cells, neighbours through L1 (best for small grids);
  *   ZMARCH    — x-y tiles marching z through a cp.async shared-memory ring (one read of
  *               each value per sweep: best once the grid outgrows L2);
- *   FUSED     — `block` sweeps per launch (2, 3, 4 or 6), temporally blocked: block 2 is
- *               the two-sweep z-marching pass (one read of pressure and divergence per two
- *               sweeps; AUTO's choice at 8 Mi cells and above), 3, 4 and 6 the 2.5-D
- *               column kernel. Fused sweeps give the same results as single sweeps (with
- *               FP16 pressure storage the intermediate sweeps are rounded as stored ones).
- *               A phase falls back to single sweeps when fusing would change which buffer
- *               holds the result.
+ *   FUSED     — two sweeps per launch (`block` 2): z-marching tiles with a one-cell ring,
+ *               one read of pressure and divergence per two sweeps (AUTO's choice at 8 Mi
+ *               cells and above). The fused sweeps give the same results as single sweeps
+ *               (with FP16 pressure storage the first sweep is rounded as a stored one). A
+ *               phase falls back to single sweeps when the fused launches would leave its
+ *               result in the other buffer of the pair (half its sweep count, rounded down,
+ *               is odd).
  * `zchunk`: z planes per CTA for ZMARCH and FUSED (0 = auto). AUTO takes RESIDENT when the
  * batch fits on chip, else by its cell count: UNBLOCKED below 8 Mi cells, FUSED with block 2
  * and 16-plane chunks below 16 Mi, FUSED with block 2 and 64-plane chunks from 16 Mi. */

@@ -1,10 +1,8 @@
-"""GPU tests of the temporally blocked Jacobi: K sweeps fused per launch must give
-bit-identical fields to K single-sweep launches in every FP32-arithmetic branch
-(warm f32, cold f32, f16 storage rounded every sweep), for grids that do and do not
-divide into the column tiles, any z chunking, and inside batches. K = 2 runs the
-two-sweep z-marching kernel (32 x 32 tiles with a one-cell ring; grids below, at and
-above one tile in x and y, chunks of 1 plane up to more than the grid), larger K the
-2.5-D column kernel."""
+"""GPU tests of the temporally blocked Jacobi: two sweeps fused per launch (the two-sweep
+z-marching kernel: 32 x 30 tiles with a one-cell ring) must give bit-identical fields to two
+single-sweep launches in every FP32-arithmetic branch (warm f32, cold f32, f16 storage
+rounded every sweep), for grids below, at and above one tile in x and y, chunks of 1 plane
+up to more than the grid, and inside batches."""
 from __future__ import annotations
 
 import numpy as np
@@ -28,10 +26,10 @@ def same(a, b):
 
 
 @pytest.mark.parametrize("mode", [A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32, A.PRESSURE_F16])
-@pytest.mark.parametrize("k,zc", [(2, 1), (2, 16), (2, 33), (3, 5), (4, 16), (4, 64), (6, 7)])
+@pytest.mark.parametrize("k,zc", [(2, 1), (2, 5), (2, 16), (2, 33)])
 @pytest.mark.parametrize("dims", [(16, 20, 24), (36, 44, 28), (64, 96, 64), (132, 20, 40)])
 def test_fused_sweeps_equal_single_sweeps(dims, k, zc, mode):
-    P = R = 12 if k != 3 else 9
+    P = R = 12
     opts = sphere_options(dims, P=P, R=R, pressure_mode=mode)
     one, fused = FireXSim(dims, opts), FireXSim(dims, opts)
     one.set_jacobi("zmarch")
@@ -41,7 +39,7 @@ def test_fused_sweeps_equal_single_sweeps(dims, k, zc, mode):
     same(one, fused)
 
 
-@pytest.mark.parametrize("k", [2, 4])
+@pytest.mark.parametrize("k", [2])
 def test_fused_zero_dt_step_matches_oracle_bit_exact(k):
     dims = (36, 44, 28)
     opts = sphere_options(dims, P=16, R=12)
@@ -53,19 +51,30 @@ def test_fused_zero_dt_step_matches_oracle_bit_exact(k):
 
 
 def test_parity_rule_falls_back_to_single_sweeps():
-    """P = 4 with k = 4 would end the solve in the other buffer: the engine must not
-    fuse that phase, and the results stay those of single sweeps."""
+    """P = 6 with two sweeps per launch (three launches) would end the solve in the other
+    buffer: the engine must not fuse that phase, and the results stay those of single
+    sweeps."""
     dims = (32, 48, 32)
-    opts = sphere_options(dims, P=4, R=8)
+    opts = sphere_options(dims, P=6, R=8)
     one, fused = FireXSim(dims, opts), FireXSim(dims, opts)
     one.set_jacobi("unblocked")
-    fused.set_jacobi("fused", 4, 16)
+    fused.set_jacobi("fused", 2, 16)
     one.step(3, DT)
     fused.step(3, DT)
     same(one, fused)
 
 
-@pytest.mark.parametrize("k", [2, 4])
+def test_fused_blocks_other_than_two_are_refused():
+    from fire_b200.sim import FireXError
+    g = FireXSim((16, 20, 24), sphere_options((16, 20, 24)))
+    for k in (3, 4, 6):
+        with pytest.raises(FireXError) as e:
+            g.set_jacobi("fused", k, 8)
+        assert e.value.code == A.ERR_BAD_ARG
+    g.close()
+
+
+@pytest.mark.parametrize("k", [2])
 def test_fused_batch_equals_single_sweep_alone(k):
     dims = [(64, 96, 64), (32, 48, 32), (36, 44, 28)]
     alone = [FireXSim(d, sphere_options(d, P=12, R=12, seed=i)) for i, d in enumerate(dims)]

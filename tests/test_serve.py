@@ -72,3 +72,46 @@ def test_admission_waits_for_memory_and_rejects_oversize():
     assert srv.poll(ib)["queue_wait_s"] > 0.0
     assert srv.used == 0 and len(srv.batch) == 0
     srv.close()
+
+
+def test_tick_budget_bounds_the_estimated_tick():
+    from fire_b200.serve import FIXED_SWEEP_EQUIVALENTS, TickBudget
+    tb = TickBudget(target_ms=10.0, initial_rate=1e6)
+    opts = make_options(pressure_iterations=20, correction_iterations=10)
+    w = TickBudget.work((10, 10, 10), opts)
+    assert w == 1000 * (30 + FIXED_SWEEP_EQUIVALENTS)
+    assert tb.fits(0.0, 1e12, members=0)  # an empty batch always takes the oldest request
+    assert tb.fits(0.0, 5e6, members=1) and not tb.fits(6e6, 5e6, members=1)
+    tb.observe(1e7, 5.0)  # measured 2e6 per ms: the estimate moves toward it
+    assert 1e6 < tb.rate < 2e6
+    for _ in range(50):
+        tb.observe(1e7, 5.0)
+    assert tb.rate == pytest.approx(2e6, rel=1e-6)
+    assert tb.fits(1e7, 0.9e7, members=3) and not tb.fits(1e7, 1.1e7, members=3)
+
+
+@pytest.mark.gpu
+def test_tick_target_admits_by_work_and_results_stay_exact():
+    """A tick target below one member's work admits one request per tick-batch: every tick
+    steps a single member, requests wait in the queue and each result equals its run alone."""
+    reqs = [_req((32, 48, 32), 3, 11), _req((16, 20, 24), 2, 12), _req((32, 40, 24), 2, 13)]
+    srv = FireXServer(tick_target_ms=1e-6)
+    ids = [srv.submit(r) for r in reqs]
+    members = []
+    while True:
+        srv._admit()
+        members.append(len(srv.slots))
+        if not srv.tick():
+            break
+    assert max(members) == 1
+    st = srv.stats()
+    assert st["completed"] == 3 and st["ticks"] == 7
+    assert st["p50_latency_s"] is not None and st["p99_latency_s"] >= st["p50_latency_s"]
+    for rid, r in zip(ids, reqs):
+        res = srv.poll(rid)
+        alone = FireXSim(r.dims, make_options(**{**r.options, "precision": A.PRECISION_MIXED}))
+        alone.step(r.steps, r.dt)
+        for f in r.keep:
+            assert np.array_equal(res["fields"][f], alone.read(f)), (r.dims, f)
+        alone.close()
+    srv.close()
