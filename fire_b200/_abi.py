@@ -53,6 +53,9 @@ JACOBI_UNBLOCKED = 1
 JACOBI_ZMARCH = 2
 JACOBI_FUSED = 3
 JACOBI_RESIDENT = 4
+STAGING_AUTO = 0
+STAGING_CPASYNC = 1
+STAGING_TMA = 2
 
 VALUE_NUMBER = 0
 VALUE_BOOLEAN = 1
@@ -147,7 +150,8 @@ class Diagnostics(C.Structure):
         ("launches_per_step", C.c_int32),
         ("jacobi_kernel", C.c_int32),
         ("jacobi_variant", C.c_int32),
-        ("reserved", C.c_int32 * 9),
+        ("jacobi_staging", C.c_int32),
+        ("reserved", C.c_int32 * 8),
     ]
 
 
@@ -204,6 +208,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_set_jacobi": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
         "firex_get_diagnostics": (C.c_int, [vp, C.POINTER(Diagnostics)]),
         "firex_batch_set_jacobi": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
+        "firex_set_staging": (C.c_int, [vp, C.c_int32]),
+        "firex_batch_set_staging": (C.c_int, [vp, C.c_int32]),
         "firex_batch_create": (C.c_int, [C.POINTER(vp)]),
         "firex_batch_destroy": (C.c_int, [vp]),
         "firex_batch_add": (C.c_int, [vp, vp]),
@@ -229,7 +235,7 @@ HEADER_SYMBOLS = [
     "firex_divergence_norm_noalloc", "firex_set_wait_limit", "firex_test_hold_face", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_preflight", "firex_stream", "firex_set_profiling", "firex_pass_times",
-    "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_batch_create", "firex_batch_destroy",
+    "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_set_staging", "firex_batch_set_staging", "firex_batch_create", "firex_batch_destroy",
     "firex_batch_add", "firex_batch_remove", "firex_batch_size", "firex_batch_step", "firex_batch_sync",
     "firex_batch_last_error", "firex_batch_stream",
 ]

@@ -9,6 +9,8 @@
 // --fmad=false (no contraction into fused multiply-add).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include <cstdint>
 #include <cuda_fp16.h>
 
@@ -175,6 +177,9 @@ struct __align__(16) FxSimDev {
     unsigned* sync;        // [2]: error word (a bounded device wait expired); from
                            // FX_RES_FLAGS: the resident Jacobi's per-box flags of both
                            // phases (zeroed at every step start)
+    int tmapOk;            // 1: tmap holds valid tensor maps (FP32 pressure)
+    int tmapPad[15];
+    CUtensorMap tmap[5];   // pressure pair, correction pair, divergence (fx_jacobi_zm2t.cuh)
 };
 
 // Work decomposition shared by every batched pass: each pass walks a flat list of

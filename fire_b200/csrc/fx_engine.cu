@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <array>
 #include <cstdlib>
 #include <cmath>
@@ -26,6 +27,8 @@
 #include "fx_jacobi_res.cuh"
 #include "fx_jacobi_zm.cuh"
 #include "fx_jacobi_zm2.cuh"
+
+static_assert(offsetof(FxSimDev, tmap) % 64 == 0, "tensor maps must sit on 64-byte boundaries");
 
 namespace {
 
@@ -130,12 +133,13 @@ struct StepPlan {
     bool row4 = false;        // single sweeps by the unblocked kernel instead
     bool fuseP = false, fuseR = false;
     bool pack = false;        // a member packs its render volumes at the end of every step
+    bool tma = false;         // the two-sweep pass stages its planes by TMA
     bool res = false;         // every sweep of a phase in one resident launch
     int resVariant = 0;       // ... by this variant of the kernel
     int resSmem = 0;          // its dynamic shared memory per CTA
     int bricks[FX_NSHAPES] = {};
     auto key() const {
-        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, res, resVariant, resSmem,
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, tma, res, resVariant, resSmem,
                         bricks[0],
                         bricks[1], bricks[2], bricks[3], bricks[4], bricks[5], bricks[6]);
     }
@@ -164,7 +168,7 @@ void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, in
     int launch = 0, sweep = 0;
     if (fuse) {
         for (; sweep + pl.k <= n; sweep += pl.k, ++launch)
-            fx_launch_jacobi_tb(st, pl.pmode, pl.k, B, pl.bricks[FX_SHAPE_COL], phase, launch, pl.zc);
+            fx_launch_jacobi_tb(st, pl.pmode, pl.k, B, pl.bricks[FX_SHAPE_COL], phase, launch, pl.zc, pl.tma);
     }
     for (; sweep < n; ++sweep, ++launch) {
         if (pl.row4) fx_launch_jacobi(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], phase, launch, sweep);
@@ -371,6 +375,7 @@ struct firex_sim {
     int device = 0;
     double named[kNumParams];
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;
+    int staging = FIREX_STAGING_AUTO;  // how the two-sweep pass stages its planes
 
     FxSimDev h{};           // host mirror of the device descriptor
     FxSimDev* d = nullptr;  // device descriptor
@@ -581,6 +586,7 @@ struct firex_batch {
     StepPlan last{};                 // plan of the most recent step (diagnostics)
     bool lastGraph = false;
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;  // batch override (AUTO: first member's)
+    int staging = FIREX_STAGING_AUTO;  // batch override of the members' staging (AUTO: first member's)
     int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
     int tableRes = -1;                               // whether resident boxes were requested
     std::vector<char> tableWater;                    // which members sprayed when the table was filled
@@ -716,13 +722,20 @@ struct firex_batch {
         if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 2 + resForce : 0) ||
             tableWater != water_signature())
             fill_table(p.k, p.zc, p.zmZc, wantRes, resForce);
+        // TMA staging of the two-sweep pass: FP32 pressure and every member's tensor maps built
+        const int staging = this->staging != FIREX_STAGING_AUTO ? this->staging : members[0]->staging;
+        bool maps = p.pmode == FX_TB_F32 && staging != FIREX_STAGING_CPASYNC;
+        for (firex_sim* s : members) maps = maps && s->h.tmapOk;
+        p.tma = p.k == 2 && maps;
         p.res = wantRes && resOk;
         if (p.res) {
             p.resSmem = resSmem;
             p.resVariant = resVariant;
             p.k = 1;
             p.fuseP = p.fuseR = false;
+            p.tma = false;
         }
+        if (p.k != 2) p.tma = false;
         for (int j = 0; j < FX_NSHAPES; ++j) p.bricks[j] = h->total[j];
         return p;
     }
@@ -1238,6 +1251,7 @@ int firex_create(const int32_t dims[3], const firex_options* opt, firex_sim** ou
         delete s;
         return FIREX_ERR_OOM;
     }
+    fx_make_tensor_maps(&h);  // without them the two-sweep pass stages by cp.async
     s->solo->members.push_back(s);
     s->solo->rebuild_table();
     int rc = s->reset();
@@ -1598,6 +1612,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     out->jacobi_variant = p.res ? p.resVariant : -1;
+    out->jacobi_staging = p.tma ? FIREX_STAGING_TMA : (p.k == 2 ? FIREX_STAGING_CPASYNC : -1);
     return FIREX_OK;
 }
 
@@ -1624,6 +1639,18 @@ int firex_batch_set_jacobi(firex_batch* b, int32_t kernel, int32_t block, int32_
     b->jacobiKernel = kernel;
     b->jacobiK = jacobi_block_kept(kernel, block);
     b->jacobiZc = zchunk;
+    return FIREX_OK;
+}
+
+int firex_set_staging(firex_sim* s, int32_t staging) {
+    if (!s || staging < FIREX_STAGING_AUTO || staging > FIREX_STAGING_CPASYNC) return FIREX_ERR_BAD_ARG;
+    s->staging = staging;
+    return FIREX_OK;
+}
+
+int firex_batch_set_staging(firex_batch* b, int32_t staging) {
+    if (!b || staging < FIREX_STAGING_AUTO || staging > FIREX_STAGING_CPASYNC) return FIREX_ERR_BAD_ARG;
+    b->staging = staging;
     return FIREX_OK;
 }
 

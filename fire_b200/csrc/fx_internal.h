@@ -22,7 +22,12 @@ void fx_launch_jacobi_zm(cudaStream_t s, bool half, const FxBatchDev* B, int bri
                          int zc);
 // K fused sweeps per launch; pmode selects the pressure storage and rounding.
 enum { FX_TB_F32 = 0, FX_TB_F16_ROUND = 1, FX_TB_F16 = 2 };
-bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc);
+// Two sweeps per launch (k = 2); with tma (FP32 pressure only) the planes are staged by TMA.
+bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc,
+                         bool tma);
+// Tensor maps of a simulation's pressure pair, correction pair and divergence for the
+// TMA-staged two-sweep pass; false when the driver refuses one (the pass then uses cp.async).
+bool fx_make_tensor_maps(FxSimDev* h);
 void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase);
 // The primary projection (phase 0) and the divergence of its result (the residual solve's
 // right-hand side) in one pass.

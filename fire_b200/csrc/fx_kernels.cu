@@ -12,12 +12,14 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 
 #include "fx_internal.h"
 #include "fx_jacobi_res.cuh"
 #include "fx_sph.cuh"
 #include "fx_jacobi_zm.cuh"
 #include "fx_jacobi_zm2.cuh"
+#include "fx_jacobi_zm2t.cuh"
 #include "fx_step_math.cuh"
 #include "fx_storage.cuh"
 
@@ -482,6 +484,46 @@ __global__ void __launch_bounds__(FX_Z2_THREADS, FX_Z2_MINB) fxk_jacobi_zm2(cons
     });
 }
 
+// ---- two Jacobi sweeps per pass, planes staged by TMA (fx_jacobi_zm2t.cuh), FP32 pressure --------
+__global__ void __launch_bounds__(FX_Z2_THREADS, FX_Z2_MINB) fxk_jacobi_zm2t(const FxBatchDev* __restrict__ B, int phase,
+                                                                int launch, int zc) {
+    extern __shared__ __align__(128) unsigned char fx_t2_dyn[];
+    // the slots must start on 128-byte boundaries: align the dynamic window (128 bytes spare)
+    FxT2Smem& sm = *reinterpret_cast<FxT2Smem*>((reinterpret_cast<uintptr_t>(fx_t2_dyn) + 127) & ~(uintptr_t)127);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < FX_T2_SLOTS; ++i) fx_mbar_init(&sm.bar[i], 1);
+        sm.err = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+    unsigned phases = 0;  // parity of each slot's next barrier phase (the same in every thread)
+    const int total = B->total[FX_SHAPE_COL];
+    int lo = 0, hi = -1, si = 0;
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        if (w < lo || w >= hi) {
+            si = fx_find_sim(B->start[FX_SHAPE_COL], B->nsims, w);
+            lo = __ldg(&B->start[FX_SHAPE_COL][si]);
+            hi = __ldg(&B->start[FX_SHAPE_COL][si + 1]);
+        }
+        const FxSimDev& S = *B->sims[si];
+        if (!S.active) continue;
+        const int b = w - lo;
+        const int ntx = (S.X + FX_Z2_TX - 1) / FX_Z2_TX, nty = (S.Y + FX_Z2_TY - 1) / FX_Z2_TY;
+        const int tx = b % ntx, ty = (b / ntx) % nty, zci = b / (ntx * nty);
+        const int z0 = zci * zc, z1 = min(S.Z, z0 + zc);
+        const FxSolveBufs bufs = fx_solve_bufs(S, phase, launch);
+        float* pout = reinterpret_cast<float*>(bufs.pout);
+        const bool ok = bufs.zeroIn
+                            ? fx_zm2t_tile<true>(S, nullptr, pout, tx * FX_Z2_TX, ty * FX_Z2_TY, z0, z1, sm, phases)
+                            : fx_zm2t_tile<false>(S, fx_t2_map_of(S, bufs.pin), pout, tx * FX_Z2_TX, ty * FX_Z2_TY, z0,
+                                                  z1, sm, phases);
+        if (!ok) {  // a barrier wait ran out: report it and stop this CTA
+            if (threadIdx.x == 0) atomicExch(S.sync + 2, 1u);
+            return;
+        }
+    }
+}
+
 // Counts the floats x for which fx_div_by_const(x, d, rcp) differs from the IEEE
 // quotient x / d (every bit pattern, 2^32 of them; any NaN matches any NaN).
 __global__ void fxk_check_div(float d, float rcp, float lo, float hi, unsigned long long* __restrict__ mismatches) {
@@ -839,10 +881,66 @@ static void launch_zm2(cudaStream_t s, const FxBatchDev* B, int bricks, int phas
     fxk_jacobi_zm2<PT, ROUND><<<bricks < g ? bricks : g, FX_Z2_THREADS, sizeof(FxZ2Smem<PT>), s>>>(B, phase, launch, zc);
 }
 
-bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time dependency on
+// the driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// A 3-D FP32 map of an X x Y x Z field (x fastest) with boxes of FX_Z2_COLS x boxY x 1 cells:
+// row stride X * 4 bytes (a multiple of 16: X is a multiple of 4), out-of-bound cells read 0.
+static bool map_field(EncodeTiledFn fn, CUtensorMap* m, void* base, int X, int Y, int Z, int boxY) {
+    const cuuint64_t dims[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
+    const cuuint64_t strides[2] = {(cuuint64_t)X * 4, (cuuint64_t)X * (cuuint64_t)Y * 4};
+    const cuuint32_t box[3] = {FX_Z2_COLS, (cuuint32_t)boxY, 1};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool fx_make_tensor_maps(FxSimDev* h) {
+    h->tmapOk = 0;
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || h->mode == FIREX_PRESSURE_F16 || (h->X & 3) != 0) return false;
+    void* bufs[4] = {h->p[0], h->p[1], h->corr[0], h->corr[1]};
+    for (int i = 0; i < 4; ++i)
+        if (!map_field(fn, &h->tmap[FX_TM_P0 + i], bufs[i], h->X, h->Y, h->Z, FX_T2_PBOX_Y)) return false;
+    if (!map_field(fn, &h->tmap[FX_TM_DIV], h->div, h->X, h->Y, h->Z, FX_T2_DBOX_Y)) return false;
+    h->tmapOk = 1;
+    return true;
+}
+
+static void launch_zm2t(cudaStream_t s, const FxBatchDev* B, int bricks, int phase, int launch, int zc) {
+    constexpr int smem = (int)sizeof(FxT2Smem) + 128;
+    static int g = [] {
+        cudaFuncSetAttribute((const void*)fxk_jacobi_zm2t, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fxk_jacobi_zm2t, FX_Z2_THREADS, smem);
+        return (per_sm > 0 ? per_sm : 1) * num_sms();
+    }();
+    fxk_jacobi_zm2t<<<bricks < g ? bricks : g, FX_Z2_THREADS, smem, s>>>(B, phase, launch, zc);
+}
+
+bool fx_launch_jacobi_tb(cudaStream_t s, int pmode, int k, const FxBatchDev* B, int bricks, int phase, int launch, int zc,
+                         bool tma) {
     switch (k) {
         case 2:  // two sweeps per pass: the z-marching form
-            if (pmode == FX_TB_F32) launch_zm2<float, false>(s, B, bricks, phase, launch, zc);
+            if (pmode == FX_TB_F32 && tma) launch_zm2t(s, B, bricks, phase, launch, zc);
+            else if (pmode == FX_TB_F32) launch_zm2<float, false>(s, B, bricks, phase, launch, zc);
             else if (pmode == FX_TB_F16_ROUND) launch_zm2<__half, true>(s, B, bricks, phase, launch, zc);
             else launch_zm2<__half, false>(s, B, bricks, phase, launch, zc);
             return true;

@@ -293,6 +293,11 @@ class FireXSim(_Handle):
         per CTA (0 = auto)."""
         self._check(self._lib.firex_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
 
+    def set_staging(self, staging: int) -> None:
+        """How the two-sweep pass stages its planes: A.STAGING_AUTO (TMA when the pressure is
+        FP32) or A.STAGING_CPASYNC."""
+        self._check(self._lib.firex_set_staging(self._h, int(staging)))
+
     @property
     def diagnostics(self) -> dict:
         d = A.Diagnostics()
@@ -364,6 +369,9 @@ class FireXBatch:
 
     def set_jacobi(self, kernel, block: int = 0, zchunk: int = 0) -> None:
         self._check(self._lib.firex_batch_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
+
+    def set_staging(self, staging: int) -> None:
+        self._check(self._lib.firex_batch_set_staging(self._h, int(staging)))
 
     def sync(self) -> None:
         self._check(self._lib.firex_batch_sync(self._h))

@@ -348,6 +348,19 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
 int firex_set_jacobi(firex_sim* sim, int32_t kernel, int32_t block, int32_t zchunk);
 int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, int32_t zchunk);
 
+/* How the two-sweep pass (FUSED, block 2) brings its pressure and divergence planes into
+ * shared memory. AUTO (the default) = TMA when the pressure is FP32: one elected thread per
+ * CTA issues tiled tensor loads (cp.async.bulk.tensor) completing on per-slot mbarriers;
+ * FP16 pressure (branch B) and CPASYNC use per-thread cp.async copies. Both give the same
+ * results bit for bit. A batch's own setting overrides its members' (AUTO: the first
+ * member's). No reference counterpart (the reference's tiled solve stages through
+ * workgroup memory, shaders.ts:405-459). */
+#define FIREX_STAGING_AUTO 0
+#define FIREX_STAGING_CPASYNC 1
+#define FIREX_STAGING_TMA 2   /* reported by firex_get_diagnostics */
+int firex_set_staging(firex_sim* sim, int32_t staging);
+int firex_batch_set_staging(firex_batch* batch, int32_t staging);
+
 /* What the engine chose for the most recent step of the simulation (or its batch). */
 typedef struct firex_diagnostics {
     int32_t fast_division;    /* 1: the Jacobi division uses the checked constant-divisor path */
@@ -357,7 +370,8 @@ typedef struct firex_diagnostics {
     int32_t launches_per_step;
     int32_t jacobi_kernel;    /* FIREX_JACOBI_* kernel the last step ran */
     int32_t jacobi_variant;   /* RESIDENT: the box variant (0-3) it ran; else -1 */
-    int32_t reserved[9];
+    int32_t jacobi_staging;   /* two-sweep pass: FIREX_STAGING_TMA or _CPASYNC it ran; else -1 */
+    int32_t reserved[8];
 } firex_diagnostics;
 int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
 
