@@ -151,7 +151,8 @@ class Diagnostics(C.Structure):
         ("jacobi_kernel", C.c_int32),
         ("jacobi_variant", C.c_int32),
         ("jacobi_staging", C.c_int32),
-        ("reserved", C.c_int32 * 8),
+        ("simulate_by", C.c_int32),
+        ("reserved", C.c_int32 * 7),
     ]
 
 
@@ -210,6 +211,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_batch_set_jacobi": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
         "firex_set_staging": (C.c_int, [vp, C.c_int32]),
         "firex_batch_set_staging": (C.c_int, [vp, C.c_int32]),
+        "firex_set_tiles": (C.c_int, [vp, C.c_int32]),
+        "firex_batch_set_tiles": (C.c_int, [vp, C.c_int32]),
         "firex_batch_create": (C.c_int, [C.POINTER(vp)]),
         "firex_batch_destroy": (C.c_int, [vp]),
         "firex_batch_add": (C.c_int, [vp, vp]),
@@ -235,7 +238,7 @@ HEADER_SYMBOLS = [
     "firex_divergence_norm_noalloc", "firex_set_wait_limit", "firex_test_hold_face", "firex_get_state",
     "firex_set_state", "firex_get_uniforms", "firex_get_info", "firex_device_bytes",
     "firex_reference_memory_estimate", "firex_preflight", "firex_stream", "firex_set_profiling", "firex_pass_times",
-    "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_set_staging", "firex_batch_set_staging", "firex_batch_create", "firex_batch_destroy",
+    "firex_planned_device_bytes", "firex_set_graphs", "firex_set_jacobi", "firex_get_diagnostics", "firex_batch_set_jacobi", "firex_set_staging", "firex_batch_set_staging", "firex_set_tiles", "firex_batch_set_tiles", "firex_batch_create", "firex_batch_destroy",
     "firex_batch_add", "firex_batch_remove", "firex_batch_size", "firex_batch_step", "firex_batch_sync",
     "firex_batch_last_error", "firex_batch_stream",
 ]

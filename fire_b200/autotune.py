@@ -1,14 +1,18 @@
-"""Jacobi autotuner: picks the Jacobi kernel and its tile parameters for a simulation or a
-batch by timing real steps on the device.
+"""Autotuner of the step's launch shapes: picks the Jacobi kernel with its tile parameters
+and plane staging, then the source pass's brick shape, for a simulation or a batch, by timing
+real steps on the device.
 
 Every Jacobi kernel of the library computes each sweep with the same FP32 operations in
 the same order (the GPU tests hold them bit-identical), so the steps taken while tuning are
 ordinary steps of the run: the trajectory is the same whichever candidate ran them. The
 candidates are the resident kernel in each box variant that fits, the single-sweep kernels
 (unblocked, and z-marching with 8, 16 or 32 planes per CTA) and the two-sweep pass with 16-,
-32- or 64-plane chunks. The winner is
-applied with set_jacobi and remembered per workload signature (grid sizes, sweep counts,
-precision, pressure branch), optionally in a JSON file so that a later process starts tuned.
+32- or 64-plane chunks, its planes staged by TMA or by cp.async. With the fastest Jacobi
+applied, the source pass's bricks (32 x 4 x 2, 32 x 2 x 4, 32 x 8 x 1 cells) are timed the
+same way; every shape computes each cell with the same operations. The winner is applied
+(set_jacobi, set_staging, set_tiles) and remembered per workload signature (grid sizes,
+sweep counts, precision, pressure branch), optionally in a JSON file so that a later process
+starts tuned.
 """
 from __future__ import annotations
 
@@ -28,17 +32,22 @@ class Candidate:
     kernel: str
     block: int = 0
     zchunk: int = 0
+    staging: int = A.STAGING_AUTO  # two-sweep pass: TMA (FP32 pressure) or cp.async
+    simulate_by: int = 0           # source-pass bricks: 32 x by x (8 / by); 0 = default
 
     def as_list(self) -> list:
-        return [self.kernel, self.block, self.zchunk]
+        return [self.kernel, self.block, self.zchunk, self.staging, self.simulate_by]
 
 
 def default_candidates() -> list:
     out = [Candidate("resident", v + 1) for v in (3, 2, 1, 0)]
     out += [Candidate("unblocked")]
     out += [Candidate("zmarch", 0, zc) for zc in (8, 16, 32)]
-    out += [Candidate("fused", 2, zc) for zc in (16, 32, 64)]
+    out += [Candidate("fused", 2, zc, st) for zc in (16, 32, 64) for st in (A.STAGING_AUTO, A.STAGING_CPASYNC)]
     return out
+
+
+SIMULATE_SHAPES = (4, 2, 8)
 
 
 def _members(target) -> list:
@@ -95,27 +104,40 @@ class JacobiTuner:
         target.sync()
         return e0.elapsed_time(e1) / self.steps
 
+    @staticmethod
+    def apply(target, c: Candidate) -> None:
+        target.set_jacobi(c.kernel, c.block, c.zchunk)
+        target.set_staging(c.staging)
+        target.set_tiles(c.simulate_by)
+
     def tune(self, target, dt: float = 1.0 / 60.0, force: bool = False) -> Candidate:
-        """Times every candidate on `target` (a FireXSim or FireXBatch) for warmup + steps
-        real steps each, applies the fastest and returns it. A cached workload is applied
-        without stepping."""
+        """Times every Jacobi candidate on `target` (a FireXSim or FireXBatch) for warmup +
+        steps real steps each, then the source pass's brick shapes with the fastest Jacobi;
+        applies the fastest combination and returns it. A cached workload is applied without
+        stepping."""
         key = signature(target)
         if key in self.cache and not force:
             best = Candidate(*self.cache[key]["choice"])
-            target.set_jacobi(best.kernel, best.block, best.zchunk)
+            self.apply(target, best)
             return best
         timings = {}
         for c in self.candidates:
-            target.set_jacobi(c.kernel, c.block, c.zchunk)
+            self.apply(target, c)
             target.step(self.warmup, dt)
             if not self._ran(target, c):
                 continue
             timings[c] = self._time(target, dt)
         if not timings:
-            target.set_jacobi("auto")
+            self.apply(target, Candidate("auto"))
             return Candidate("auto")
         best = min(timings, key=timings.get)
-        target.set_jacobi(best.kernel, best.block, best.zchunk)
+        for by in SIMULATE_SHAPES:
+            c = Candidate(best.kernel, best.block, best.zchunk, best.staging, by)
+            self.apply(target, c)
+            target.step(self.warmup, dt)
+            timings[c] = self._time(target, dt)
+        best = min(timings, key=timings.get)
+        self.apply(target, best)
         self.last_timings = {json.dumps(c.as_list()): ms for c, ms in timings.items()}
         self.cache[key] = {"choice": best.as_list(), "ms_per_step": timings[best], "timings": self.last_timings}
         self._save()

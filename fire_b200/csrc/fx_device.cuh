@@ -202,14 +202,14 @@ enum FxShape {
 struct FxResBox {
     int by, bz, nby, nbz;
 };
-// CELL: 32 x 4 x 2 cells, one thread per cell (simulate).
+// CELL: 32 x BY x (8 / BY) cells, one thread per cell (simulate); BY = FX_CELL_BY unless
+//       the plan tunes it (firex_set_tiles).
 // ROW4: 256 groups of 4 consecutive x cells in memory order (stencils).
 // COL : tiles x z chunks of the two-sweep Jacobi pass (see fx_jacobi_zm2.cuh).
 // ZM  : z-marching tiles of the single-sweep Jacobi (see fx_jacobi_zm.cuh).
 // TAB : 256 entries of the per-step tables of simulate.
 #define FX_CELL_BX 32
 #define FX_CELL_BY 4
-#define FX_CELL_BZ 2
 #define FX_ROW4_THREADS 256
 #define FX_SPH_THREADS 256                    // threads of the droplet passes: one warp per droplet
 #define FX_SPH_DROPLETS (FX_SPH_THREADS / 32)  // droplets per brick

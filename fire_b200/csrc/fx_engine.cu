@@ -113,10 +113,12 @@ float host_jitter(uint64_t seed, int64_t f, float a) {
     return 1.0f + a * (2.0f * u - 1.0f);
 }
 
-long long bricks_cell(int X, int Y, int Z) {
-    return (long long)((X + FX_CELL_BX - 1) / FX_CELL_BX) * ((Y + FX_CELL_BY - 1) / FX_CELL_BY) *
-           ((Z + FX_CELL_BZ - 1) / FX_CELL_BZ);
+// Bricks of the source pass: 32 x by x (8 / by) cells.
+long long bricks_cell(int X, int Y, int Z, int by) {
+    const int bz = 256 / (FX_CELL_BX * by);
+    return (long long)((X + FX_CELL_BX - 1) / FX_CELL_BX) * ((Y + by - 1) / by) * ((Z + bz - 1) / bz);
 }
+bool sim_by_ok(int by) { return by == 0 || by == 2 || by == 4 || by == 8; }
 long long bricks_row4(int X, int Y, int Z) {
     long long groups = (long long)(X / 4) * Y * Z;
     return (groups + FX_ROW4_THREADS - 1) / FX_ROW4_THREADS;
@@ -134,12 +136,14 @@ struct StepPlan {
     bool fuseP = false, fuseR = false;
     bool pack = false;        // a member packs its render volumes at the end of every step
     bool tma = false;         // the two-sweep pass stages its planes by TMA
+    int simBy = FX_CELL_BY;   // source-pass bricks: 32 x simBy x (8 / simBy) cells
     bool res = false;         // every sweep of a phase in one resident launch
     int resVariant = 0;       // ... by this variant of the kernel
     int resSmem = 0;          // its dynamic shared memory per CTA
     int bricks[FX_NSHAPES] = {};
     auto key() const {
-        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, tma, res, resVariant, resSmem,
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, tma, simBy, res, resVariant,
+                        resSmem,
                         bricks[0],
                         bricks[1], bricks[2], bricks[3], bricks[4], bricks[5], bricks[6]);
     }
@@ -183,7 +187,7 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     fx_launch_step_begin(st, B);
     fx_launch_step_tables(st, B, pl.bricks[FX_SHAPE_TAB]);
     if (sph_launches(pl)) fx_launch_sph(st, B, pl.bricks[FX_SHAPE_ROW4], pl.bricks[FX_SHAPE_PART]);
-    fx_launch_simulate(st, pl.storage, B, pl.bricks[FX_SHAPE_CELL]);
+    fx_launch_simulate(st, pl.storage, pl.simBy, B, pl.bricks[FX_SHAPE_CELL]);
     fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 0);
     enqueue_jacobi_phase(st, pl, B, 0);
     fx_launch_project_div(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4]);
@@ -376,6 +380,7 @@ struct firex_sim {
     double named[kNumParams];
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;
     int staging = FIREX_STAGING_AUTO;  // how the two-sweep pass stages its planes
+    int simBy = 0;                     // source-pass brick height (0: FX_CELL_BY)
 
     FxSimDev h{};           // host mirror of the device descriptor
     FxSimDev* d = nullptr;  // device descriptor
@@ -587,7 +592,9 @@ struct firex_batch {
     bool lastGraph = false;
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;  // batch override (AUTO: first member's)
     int staging = FIREX_STAGING_AUTO;  // batch override of the members' staging (AUTO: first member's)
+    int simBy = 0;                     // batch override of the source-pass bricks (0: first member's)
     int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
+    int tableSimBy = -1;
     int tableRes = -1;                               // whether resident boxes were requested
     std::vector<char> tableWater;                    // which members sprayed when the table was filled
     bool resOk = false;                              // ... and the batch fits one resident launch
@@ -617,7 +624,7 @@ struct firex_batch {
 
     // Fills the brick prefix sums for the launch shape (k, zc); resident boxes when wanted,
     // of variant resForce when that is 0-3.
-    void fill_table(int k, int zc, int zmZc, bool wantRes, int resForce) {
+    void fill_table(int k, int zc, int zmZc, bool wantRes, int resForce, int simBy) {
         int acc[FX_NSHAPES] = {};
         h->nsims = (int)members.size();
         std::vector<FxResBox> boxes;
@@ -653,7 +660,7 @@ struct firex_batch {
                 acc[FX_SHAPE_RES] += boxes[i].nby * boxes[i].nbz;
             }
             acc[FX_SHAPE_TAB] += (fx_tab_layout(s->X, s->Y, s->Z).total + 255) / 256;
-            acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z);
+            acc[FX_SHAPE_CELL] += (int)bricks_cell(s->X, s->Y, s->Z, simBy);
             acc[FX_SHAPE_ROW4] += (int)bricks_row4(s->X, s->Y, s->Z);
             acc[FX_SHAPE_COL] += k == 2 ? fx_zm2_bricks(s->X, s->Y, s->Z, zc) : 0;
             acc[FX_SHAPE_ZM] += fx_zm_bricks(s->X, s->Y, s->Z, zmZc);
@@ -663,6 +670,7 @@ struct firex_batch {
             h->total[j] = acc[j];
         }
         tableK = k;
+        tableSimBy = simBy;
         tableZc = zc;
         tableZmZc = zmZc;
         tableRes = wantRes ? 2 + resForce : 0;
@@ -719,9 +727,11 @@ struct firex_batch {
         if (!p.fuseP && !p.fuseR) p.k = 1;
         p.row4 = kernel == FIREX_JACOBI_UNBLOCKED;
         p.zmZc = (kernel == FIREX_JACOBI_ZMARCH && zc > 0) ? zc : zm_chunk(zm32, zm16);
+        const int by = this->simBy ? this->simBy : members[0]->simBy;
+        p.simBy = by ? by : FX_CELL_BY;
         if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 2 + resForce : 0) ||
-            tableWater != water_signature())
-            fill_table(p.k, p.zc, p.zmZc, wantRes, resForce);
+            tableWater != water_signature() || tableSimBy != p.simBy)
+            fill_table(p.k, p.zc, p.zmZc, wantRes, resForce, p.simBy);
         // TMA staging of the two-sweep pass: FP32 pressure and every member's tensor maps built
         const int staging = this->staging != FIREX_STAGING_AUTO ? this->staging : members[0]->staging;
         bool maps = p.pmode == FX_TB_F32 && staging != FIREX_STAGING_CPASYNC;
@@ -789,7 +799,7 @@ struct firex_batch {
             fx_launch_sph(stream, d, pl.bricks[FX_SHAPE_ROW4], pl.bricks[FX_SHAPE_PART]);
             mark(FIREX_PASS_PARTICLES, sph_launches(pl));
         }
-        fx_launch_simulate(stream, pl.storage, d, pl.bricks[FX_SHAPE_CELL]);
+        fx_launch_simulate(stream, pl.storage, pl.simBy, d, pl.bricks[FX_SHAPE_CELL]);
         mark(FIREX_PASS_SIMULATE, 1);
         fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 0);
         mark(FIREX_PASS_DIVERGENCE, 1);
@@ -1613,6 +1623,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     out->jacobi_variant = p.res ? p.resVariant : -1;
     out->jacobi_staging = p.tma ? FIREX_STAGING_TMA : (p.k == 2 ? FIREX_STAGING_CPASYNC : -1);
+    out->simulate_by = p.simBy;
     return FIREX_OK;
 }
 
@@ -1651,6 +1662,18 @@ int firex_set_staging(firex_sim* s, int32_t staging) {
 int firex_batch_set_staging(firex_batch* b, int32_t staging) {
     if (!b || staging < FIREX_STAGING_AUTO || staging > FIREX_STAGING_CPASYNC) return FIREX_ERR_BAD_ARG;
     b->staging = staging;
+    return FIREX_OK;
+}
+
+int firex_set_tiles(firex_sim* s, int32_t simulate_by) {
+    if (!s || !sim_by_ok(simulate_by)) return FIREX_ERR_BAD_ARG;
+    s->simBy = simulate_by;
+    return FIREX_OK;
+}
+
+int firex_batch_set_tiles(firex_batch* b, int32_t simulate_by) {
+    if (!b || !sim_by_ok(simulate_by)) return FIREX_ERR_BAD_ARG;
+    b->simBy = simulate_by;
     return FIREX_OK;
 }
 

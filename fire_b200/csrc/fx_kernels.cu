@@ -93,13 +93,16 @@ struct Acc {
     FXD uint32_t liquid(int i) const { return __ldg(liq + i); }
 };
 
-template <class St>
+// One thread per cell of a 32 x BY x (8 / BY) brick (BY = 2, 4 or 8: the tunable brick
+// shape; FX_CELL_BY, 4, by default).
+template <class St, int BY>
 __global__ void __launch_bounds__(256, 3) fxk_simulate(const FxBatchDev* __restrict__ B) {
+    constexpr int BX = FX_CELL_BX, BZ = 256 / (FX_CELL_BX * BY);
     fx_for_bricks<FX_SHAPE_CELL>(B, [&](const FxSimDev& S, int b) {
-        const int nbx = (S.X + FX_CELL_BX - 1) / FX_CELL_BX, nby = (S.Y + FX_CELL_BY - 1) / FX_CELL_BY;
-        const int x = (b % nbx) * FX_CELL_BX + threadIdx.x % FX_CELL_BX;
-        const int y = ((b / nbx) % nby) * FX_CELL_BY + (threadIdx.x / FX_CELL_BX) % FX_CELL_BY;
-        const int z = (b / (nbx * nby)) * FX_CELL_BZ + threadIdx.x / (FX_CELL_BX * FX_CELL_BY);
+        const int nbx = (S.X + BX - 1) / BX, nby = (S.Y + BY - 1) / BY;
+        const int x = (b % nbx) * BX + threadIdx.x % BX;
+        const int y = ((b / nbx) % nby) * BY + (threadIdx.x / BX) % BY;
+        const int z = (b / (nbx * nby)) * BZ + threadIdx.x / (BX * BY);
         if (x >= S.X || y >= S.Y || z >= S.Z) return;
         const FxGrid g{S.X, S.Y, S.Z};
         Acc<St> a{S.flow[S.fi], S.species[S.si], S.liquid};
@@ -824,14 +827,22 @@ void fx_launch_step_tables(cudaStream_t s, const FxBatchDev* B, int bricks) {
     fxk_step_tables<<<bricks > 0 ? bricks : 1, 256, 0, s>>>(B);
 }
 
-void fx_launch_simulate(cudaStream_t s, int storage, const FxBatchDev* B, int bricks) {
-    if (storage == FX_STORAGE_MIXED) {
-        static int g = persistent_grid((const void*)fxk_simulate<StMixed>, 256, 1 << 30);
-        fxk_simulate<StMixed><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
-    } else {
-        static int g = persistent_grid((const void*)fxk_simulate<StF32>, 256, 1 << 30);
-        fxk_simulate<StF32><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
-    }
+template <class St, int BY>
+static void launch_simulate(cudaStream_t s, const FxBatchDev* B, int bricks) {
+    static int g = persistent_grid((const void*)fxk_simulate<St, BY>, 256, 1 << 30);
+    fxk_simulate<St, BY><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
+}
+
+template <class St>
+static void launch_simulate_shape(cudaStream_t s, int by, const FxBatchDev* B, int bricks) {
+    if (by == 2) launch_simulate<St, 2>(s, B, bricks);
+    else if (by == 8) launch_simulate<St, 8>(s, B, bricks);
+    else launch_simulate<St, 4>(s, B, bricks);
+}
+
+void fx_launch_simulate(cudaStream_t s, int storage, int by, const FxBatchDev* B, int bricks) {
+    if (storage == FX_STORAGE_MIXED) launch_simulate_shape<StMixed>(s, by, B, bricks);
+    else launch_simulate_shape<StF32>(s, by, B, bricks);
 }
 
 void fx_launch_divergence(cudaStream_t s, const FxBatchDev* B, int bricks, int phase) {

@@ -3,6 +3,7 @@
     python -m fire_b200.run_case X Y Z [--steps N] [--jacobi auto|unblocked|zmarch|fused|resident]
                                        [--block K] [--zchunk ZC] [--pressure auto|warm_f32|f16|cold_f32]
                                        [--mixed] [--iters P R] [--profile] [--time N]
+                                       [--staging auto|cpasync]
 
 A sphere emitter near the floor (radius X/9), seeded velocity noise and emission jitter,
 dt = 1/60. Used as the command under profilers (one process, one GPU, small cases).
@@ -33,6 +34,8 @@ def main() -> None:
     ap.add_argument("--iters", type=int, nargs=2, default=(96, 96))
     ap.add_argument("--profile", action="store_true", help="per-pass device times (no graph replay)")
     ap.add_argument("--time", type=int, default=0, help="then time this many steps (graph replay)")
+    ap.add_argument("--staging", default="auto", choices=["auto", "cpasync"],
+                    help="plane staging of the two-sweep pass (auto: TMA with FP32 pressure)")
     a = ap.parse_args()
     X, Y, Z = a.dims
     opts = make_options(pressure_iterations=a.iters[0], correction_iterations=a.iters[1], seed=1, velocity_noise=0.05,
@@ -41,6 +44,7 @@ def main() -> None:
                         spheres=[dict(center=(X / 2, Y / 16, Z / 2), radius=X / 9)])
     s = FireXSim((X, Y, Z), opts)
     s.set_jacobi(a.jacobi, a.block, a.zchunk)
+    s.set_staging(A.STAGING_CPASYNC if a.staging == "cpasync" else A.STAGING_AUTO)
     if a.profile:
         s.set_profiling(True)
         s.pass_times()

@@ -298,6 +298,11 @@ class FireXSim(_Handle):
         FP32) or A.STAGING_CPASYNC."""
         self._check(self._lib.firex_set_staging(self._h, int(staging)))
 
+    def set_tiles(self, simulate_by: int) -> None:
+        """Brick shape of the source pass: 32 x simulate_by x (8 / simulate_by) cells (2, 4, 8;
+        0: default)."""
+        self._check(self._lib.firex_set_tiles(self._h, int(simulate_by)))
+
     @property
     def diagnostics(self) -> dict:
         d = A.Diagnostics()
@@ -372,6 +377,9 @@ class FireXBatch:
 
     def set_staging(self, staging: int) -> None:
         self._check(self._lib.firex_batch_set_staging(self._h, int(staging)))
+
+    def set_tiles(self, simulate_by: int) -> None:
+        self._check(self._lib.firex_batch_set_tiles(self._h, int(simulate_by)))
 
     def sync(self) -> None:
         self._check(self._lib.firex_batch_sync(self._h))

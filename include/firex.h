@@ -361,6 +361,13 @@ int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, in
 int firex_set_staging(firex_sim* sim, int32_t staging);
 int firex_batch_set_staging(firex_batch* batch, int32_t staging);
 
+/* Brick shape of the source pass (simulate, shaders.ts:151-342): one thread per cell of a
+ * 32 x simulate_by x (8 / simulate_by) brick, simulate_by = 2, 4 (the default) or 8; 0 restores
+ * the default. The shapes give identical results; fire_b200/autotune.py times them. A batch's
+ * own setting overrides its members' (0: the first member's). */
+int firex_set_tiles(firex_sim* sim, int32_t simulate_by);
+int firex_batch_set_tiles(firex_batch* batch, int32_t simulate_by);
+
 /* What the engine chose for the most recent step of the simulation (or its batch). */
 typedef struct firex_diagnostics {
     int32_t fast_division;    /* 1: the Jacobi division uses the checked constant-divisor path */
@@ -371,7 +378,8 @@ typedef struct firex_diagnostics {
     int32_t jacobi_kernel;    /* FIREX_JACOBI_* kernel the last step ran */
     int32_t jacobi_variant;   /* RESIDENT: the box variant (0-3) it ran; else -1 */
     int32_t jacobi_staging;   /* two-sweep pass: FIREX_STAGING_TMA or _CPASYNC it ran; else -1 */
-    int32_t reserved[8];
+    int32_t simulate_by;      /* source-pass bricks of 32 x simulate_by x (8 / simulate_by) cells */
+    int32_t reserved[7];
 } firex_diagnostics;
 int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
 
