@@ -11,9 +11,9 @@
 // shaders.ts:1-512 and pressureShaders.ts:1-161 in the dispatch order of
 // FireXEngine.ts:2115-2276, and tests/test_reference_golden.py requires this restatement to
 // reproduce those fixtures bit for bit (all three pressure branches, reset and developed
-// states, dt = 0, 1/60, 1/30, a non-default parameter set). The contracts the reference's
-// tests assert are re-asserted by tests/test_oracle_contracts.py. The droplet passes are
-// pinned against a numpy restatement only (tests/test_sph.py).
+// states, dt = 0, 1/60, 1/30, a non-default parameter set, the SPH droplet passes of
+// shaders.ts:514-825 with both nozzles and the spray switched off). The contracts the
+// reference's tests assert are re-asserted by tests/test_oracle_contracts.py.
 //
 // Arithmetic conventions (shared with the CUDA kernels, which must match them):
 //   * every WGSL expression is evaluated left to right in the precision T with no fused

@@ -30,18 +30,26 @@ from tests.golden.reference_step import ReferenceStep, load_programs  # noqa: E4
 
 OUT = HERE / "reference_steps.npz"
 
+# name, dims, branch, P, R, start, steps (dt per step), parameters, cinematic, droplets,
+# parameter changes before given steps
 CASES = [
-    # name, dims, branch, P, R, start, steps (dt per step), parameters, cinematic
-    ("reset_A", (8, 12, 8), "A", 6, 6, "reset", [1 / 60] * 3, {}, 1),
-    ("developed_A", (12, 16, 8), "A", 5, 5, "developed", [1 / 60, 1 / 60], {}, 1),
-    ("developed_B", (12, 16, 8), "B", 5, 5, "developed", [1 / 60, 1 / 60], {}, 1),
-    ("developed_C", (12, 16, 8), "C", 5, 5, "developed", [1 / 60, 1 / 60], {}, 1),
-    ("dt_zero_and_large", (8, 12, 12), "A", 4, 3, "developed", [0.0, 1 / 30], {}, 1),
+    ("reset_A", (8, 12, 8), "A", 6, 6, "reset", [1 / 60] * 3, {}, 1, 0, {}),
+    ("developed_A", (12, 16, 8), "A", 5, 5, "developed", [1 / 60, 1 / 60], {}, 1, 0, {}),
+    ("developed_B", (12, 16, 8), "B", 5, 5, "developed", [1 / 60, 1 / 60], {}, 1, 0, {}),
+    ("developed_C", (12, 16, 8), "C", 5, 5, "developed", [1 / 60, 1 / 60], {}, 1, 0, {}),
+    ("dt_zero_and_large", (8, 12, 12), "A", 4, 3, "developed", [0.0, 1 / 30], {}, 1, 0, {}),
     ("parameters", (8, 16, 12), "A", 4, 4, "developed", [1 / 60, 1 / 60],
      dict(firePower=3.7, vorticity=5.0, buoyancyScale=3.1, sourceLift=2.4, flamePersistence=0.8,
           airEntrainment=2.6, domainWidth=2.0, domainHeight=3.0, domainDepth=1.5, sourceThickness=2.2,
-          burnerSize=1.2, burnerDepth=0.9, heatEfficiency=0.5, fuelRate=0.6, oxygenRate=0.8, aimHeight=0.7), 0),
-    ("odd_iterations", (12, 8, 16), "A", 3, 1, "developed", [1 / 60, 1 / 60, 1 / 60], {}, 1),
+          burnerSize=1.2, burnerDepth=0.9, heatEfficiency=0.5, fuelRate=0.6, oxygenRate=0.8, aimHeight=0.7), 0, 0, {}),
+    ("odd_iterations", (12, 8, 16), "A", 3, 1, "developed", [1 / 60, 1 / 60, 1 / 60], {}, 1, 0, {}),
+    # droplets: the jet and the spray nozzle (shaders.ts:514-825), spray switched off before
+    # the last step (the state machine parks the droplets and clears the liquid field)
+    ("water_jet", (12, 16, 16), "A", 4, 4, "developed", [1 / 60] * 3,
+     dict(waterEnabled=True, waterFlow=1.0, nozzleType=0), 1, 96, {}),
+    ("water_spray_then_off", (12, 16, 16), "A", 4, 4, "developed", [1 / 60] * 3,
+     dict(waterEnabled=True, waterFlow=0.6, nozzleType=1, sprayAngle=24, aimHeight=0.55), 1, 128,
+     {2: dict(waterEnabled=False)}),
 ]
 
 
@@ -63,8 +71,9 @@ def developed_state(dims, seed):
     return flow, species, pressure, liquid
 
 
-def run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, seed):
-    sim = ReferenceStep(progs, dims, branch=branch, P=P, R=R, parameters=params, cinematic=cinematic)
+def run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, droplets, changes, seed):
+    sim = ReferenceStep(progs, dims, branch=branch, P=P, R=R, parameters=params, cinematic=cinematic,
+                        particle_count=droplets)
     rec = {}
     if start == "developed":
         flow, species, pressure, liquid = developed_state(dims, seed)
@@ -79,6 +88,7 @@ def run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, see
     for k, v in init.items():
         rec[f"{name}/in/{k}"] = v
     for i, dt in enumerate(dts):
+        sim.par.update(changes.get(i, {}))
         trace = {}
         sim.step(dt, trace)
         cur = sim.current()
@@ -86,7 +96,8 @@ def run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, see
         for k, v in cur.items():
             rec[f"{name}/step{i}/{k}"] = v
     meta = dict(dims=list(dims), branch=branch, P=P, R=R, start=start, dts=dts, parameters=params,
-                cinematic=cinematic, start_time=0.35 if start == "developed" else 0.0,
+                cinematic=cinematic, droplets=droplets, changes={str(k): v for k, v in changes.items()},
+                start_time=0.35 if start == "developed" else 0.0,
                 start_frame=21 if start == "developed" else 0,
                 final=dict(simulation_time=sim.simulation_time, frame_index=sim.frame_index,
                            species_index=sim.species_index, pressure_index=sim.pressure_index))
@@ -96,11 +107,12 @@ def run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, see
 def main(reference_root: str) -> None:
     progs = load_programs(reference_root)
     arrays, metas = {}, {}
-    for k, (name, dims, branch, P, R, start, dts, params, cinematic) in enumerate(CASES):
-        rec, meta = run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, seed=1000 + k)
+    for k, (name, dims, branch, P, R, start, dts, params, cinematic, droplets, changes) in enumerate(CASES):
+        rec, meta = run_case(progs, name, dims, branch, P, R, start, dts, params, cinematic, droplets, changes,
+                             seed=1000 + k)
         arrays.update(rec)
         metas[name] = meta
-        print(f"{name}: {dims} branch {branch}, {len(dts)} steps")
+        print(f"{name}: {dims} branch {branch}, {len(dts)} steps, {droplets} droplets")
     arrays["meta"] = np.frombuffer(json.dumps(metas, sort_keys=True).encode(), np.uint8)
     np.savez_compressed(OUT, **arrays)
     print(f"wrote {OUT} ({OUT.stat().st_size} bytes)")

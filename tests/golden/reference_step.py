@@ -6,7 +6,12 @@ The shaders are the reference's text, parsed and evaluated by tests/golden/wgsl_
   * FIREX_COMPUTE_WGSL     src/sim/firex/shaders.ts:1-512 (initializeFields, simulate,
     computeDivergence, solvePressureGlobal, solvePressureTiled, projectVelocity, copyFlow);
   * FIREX_F16_PRESSURE_WGSL src/sim/firex/pressureShaders.ts:1-161 (solvePressureF16Tiled,
-    projectVelocityF16).
+    projectVelocityF16);
+  * FIREX_PARTICLE_WGSL    src/sim/firex/shaders.ts:514-825 (computeParticleDensity,
+    integrateParticles, depositParticles), with sin / cos / tan / exp evaluated in double
+    precision and rounded to f32 (hash11 scales one ULP of sin by 43758, so the droplets
+    depend on which correctly-bounded sin is used: this is the choice the library and its
+    oracle make).
 
 The host side around them is restated here from src/sim/firex/FireXEngine.ts (the reference
 host is TypeScript driving WebGPU, which cannot run on this machine):
@@ -19,7 +24,11 @@ host is TypeScript driving WebGPU, which cannot run on this machine):
     :422-451) and the 8-float f16 pressure block;
   * encodeSimulationStep (:2115-2276) with its three pressure branches, ping-pong indices,
     buffer clears and dispatch sizes; the step then advances simulationTime and frameIndex
-    (renderOfflineFrameInternal :669-682).
+    (renderOfflineFrameInternal :669-682);
+  * the droplet state machine of encodeSimulationStep (:2158-2171: spray on -> initial
+    droplets if parked, liquid cleared, density / integration / deposition over the
+    particle bind group (:1772-1786), ping-pong; spray off -> liquid cleared and droplets
+    parked) and writeParticleInitialState (:1976-2034, JavaScript doubles stored as f32).
 Branch choice: the reference takes the heavy branches (B: f16 tiled, C: f32 tiled, cold
 start) only from 64 Mi cells (:2175); `branch` forces one on a small grid so every branch's
 kernels and bookkeeping run here.
@@ -47,17 +56,26 @@ DEFAULT_PARAMETERS = dict(
 
 def load_programs(reference_root):
     root = Path(reference_root)
-    main = Program(wgsl_from_ts((root / SHADERS).read_text(), "FIREX_COMPUTE_WGSL"))
+    src = (root / SHADERS).read_text()
+    main = Program(wgsl_from_ts(src, "FIREX_COMPUTE_WGSL"))
     f16 = Program(wgsl_from_ts((root / PRESSURE_SHADERS).read_text(), "FIREX_F16_PRESSURE_WGSL"))
-    return main, f16
+    particles = Program(wgsl_from_ts(src, "FIREX_PARTICLE_WGSL"), transcendentals="f64")
+    return main, f16, particles
 
 
 class ReferenceStep:
     """One Fire-X simulation run by the reference's kernels. Fields are numpy arrays in the
     reference's buffer layout (cell index x + X*(y + Y*z))."""
 
-    def __init__(self, programs, dims, branch="A", P=8, R=8, parameters=None, cinematic=1, time_step=1 / 60):
-        self.main, self.f16 = programs
+    def __init__(self, programs, dims, branch="A", P=8, R=8, parameters=None, cinematic=1, time_step=1 / 60,
+                 particle_count=0):
+        self.main, self.f16, self.sph = programs
+        self.np = int(particle_count)
+        self.particles = [np.zeros((self.np, 8), np.float32) for _ in range(2)]
+        self.density = np.zeros((self.np, 4), np.float32)
+        self.particle_index = 0
+        self.particle_field_active = False
+        self.liquid_may_contain_water = False
         self.X, self.Y, self.Z = dims
         self.N = self.X * self.Y * self.Z
         self.branch = branch
@@ -85,15 +103,15 @@ class ReferenceStep:
     # ---- uniforms
     def uniforms(self, dt):
         """writeUniforms (FireXEngine.ts:2043-2113). Presentation-only slots (canvas size and
-        aspect, ray steps, particle count, configuration.timeStep) do not enter the compute
-        kernels; they hold 1, 1, 1, 0, 0 and `time_step`."""
+        aspect, ray steps, configuration.timeStep) do not enter the compute kernels; they
+        hold 1, 1, 1, 0 and `time_step`."""
         p = self.par
         u = [self.X, self.Y, self.Z, self.N,
              dt, self.simulation_time, self.frame_index, self.time_step,
              p["fuelRate"], p["oxygenRate"], p["heatEfficiency"], p["vorticity"],
              p["waterFlow"], (p["sprayAngle"] * math.pi) / 180, 1 if p["waterEnabled"] else 0, 300,
              p["cameraYaw"], p["cameraPitch"], p["cameraDistance"], 1,
-             1, 1, 0, 0,
+             1, 1, 0, self.np,
              p["viewMode"], p["aimHeight"], p["nozzleType"], p["exposure"],
              p["burnerSize"], p["burnerDepth"], p["sourceThickness"], p["firePower"],
              p["domainWidth"], p["domainHeight"], p["domainDepth"], 0,
@@ -155,6 +173,79 @@ class ReferenceStep:
         gy = math.ceil(total / gx)
         f, s, p = self.flow, self.species, self.pressure
         self._run("initializeFields", self._group(f[1], s[1], f[0], s[0], p[0], p[1]), (gx, gy, 1), u)
+        self.particles = [np.zeros((self.np, 8), np.float32) for _ in range(2)]
+        self.density = np.zeros((self.np, 4), np.float32)
+        self.write_particle_initial_state(self.water_active())
+        self.liquid_may_contain_water = False
+
+    # ---- droplets
+    def water_active(self):
+        return bool(self.par["waterEnabled"]) and self.par["waterFlow"] > 0.001  # FireXEngine.ts:2537-2539
+
+    def write_particle_initial_state(self, active):
+        """writeParticleInitialState (FireXEngine.ts:1976-2034): JavaScript doubles, stored as
+        f32 (Float32Array) at the end."""
+        p = self.par
+        out = np.zeros((self.np, 8), np.float64)
+        aim_x = (0.52 - 0.035) * p["domainWidth"]
+        aim_y = (p["aimHeight"] - 0.5) * p["domainHeight"]
+        aim_len = math.hypot(aim_x, aim_y)
+        base = (aim_x / aim_len, aim_y / aim_len, 0.0)
+        tangent = (base[1], -base[0], 0.0)
+
+        def hsh(v):
+            h = math.sin(v * 12.9898 + 1.317) * 43758.5453
+            return h - math.floor(h)
+
+        spray = p["nozzleType"] >= 0.5
+        for i in range(self.np):
+            phase = i / self.np
+            angle = hsh(i * 3.771 + 4.91) * math.pi * 2
+            radial = math.sqrt(hsh(i * 3.771 + 0.17))
+            cone = math.tan((p["sprayAngle"] * math.pi) / 180) * radial * (0.72 if spray else 0.1)
+            disk_x, disk_y, disk_z = tangent[0] * math.cos(angle), tangent[1] * math.cos(angle), -math.sin(angle)
+            dx, dy, dz = base[0] + disk_x * cone, base[1] + disk_y * cone, disk_z * cone
+            dl = math.hypot(dx, dy, dz)
+            dx, dy, dz = dx / dl, dy / dl, dz / dl
+            var = 0.24 if spray else 0.05
+            speed = (0.82 + p["waterFlow"] * 0.82) * (1 - var * 0.5 + hsh(i * 3.771 + 9.37) * var)
+            age = phase * 0.72
+            origin_r = 0.006 if spray else 0.0028
+            out[i, 0] = 0.035 + (disk_x * radial * origin_r + dx * speed * age) / p["domainWidth"]
+            out[i, 1] = max(0.012, 0.5 + (disk_y * radial * origin_r + dy * speed * age - 0.29 * age * age)
+                            / p["domainHeight"])
+            out[i, 2] = 0.5 + (disk_z * radial * origin_r + dz * speed * age) / p["domainDepth"]
+            out[i, 3] = age if active else -phase * 0.72
+            if active:
+                out[i, 4:8] = (dx * speed, dy * speed - 0.58 * age, dz * speed, 0.52 + p["waterFlow"] * 0.88)
+        init = out.astype(np.float32)
+        self.particles = [init.copy(), init.copy()]
+        self.particle_index = 0
+        self.particle_field_active = active
+
+    def _particle_pass(self, u):
+        """FireXEngine.ts:2158-2171 and the particle bind groups (:1772-1786)."""
+        if self.water_active():
+            if not self.particle_field_active:
+                self.write_particle_initial_state(True)
+            self.liquid[...] = 0
+            i = self.particle_index
+            prog = self.sph
+            prog.bind("flowField", self.flow[0])
+            prog.bind("particlesIn", self.particles[i])
+            prog.bind("particlesOut", self.particles[1 - i])
+            prog.bind("densityData", self.density)
+            prog.bind("liquidField", self.liquid)
+            prog.bind_uniform("params", u)
+            groups = (math.ceil(self.np / 64), 1, 1)
+            for entry in ("computeParticleDensity", "integrateParticles", "depositParticles"):
+                prog.run(entry, groups)
+            self.particle_index = 1 - i
+            self.liquid_may_contain_water = True
+        elif self.liquid_may_contain_water or self.particle_field_active:
+            self.liquid[...] = 0
+            self.write_particle_initial_state(False)
+            self.liquid_may_contain_water = False
 
     # ---- encodeSimulationStep (FireXEngine.ts:2115-2276) and the counters (:669-682)
     def step(self, dt, trace=None):
@@ -163,6 +254,8 @@ class ReferenceStep:
         f, s, p, c = self.flow, self.species, self.pressure, self.correction
         X, Y, Z = self.X, self.Y, self.Z
         rec = (lambda name, arr: trace.__setitem__(name, arr.copy())) if trace is not None else (lambda *a: None)
+        if self.np > 0:
+            self._particle_pass(u)
         si = self.species_index
         sim_group = (self._group(f[0], s[0], f[1], s[1], p[0], self.reaction) if si == 0 else
                      self._group(f[0], s[1], f[1], s[0], p[0], self.reaction))
@@ -241,6 +334,9 @@ class ReferenceStep:
 
     # ---- the resident state, in the order of the library's field ids
     def current(self):
-        return dict(flow=self.flow[0].copy(), species=self.species[self.species_index].copy(),
-                    pressure=self.pressure[self.pressure_index].astype(np.float32),
-                    divergence=self.divergence.copy(), reaction=self.reaction.copy(), liquid=self.liquid.copy())
+        out = dict(flow=self.flow[0].copy(), species=self.species[self.species_index].copy(),
+                   pressure=self.pressure[self.pressure_index].astype(np.float32),
+                   divergence=self.divergence.copy(), reaction=self.reaction.copy(), liquid=self.liquid.copy())
+        if self.np > 0:
+            out["particles"] = self.particles[self.particle_index].copy()
+        return out

@@ -15,8 +15,9 @@ allows a range of results:
     operations with round-to-nearest-even (the specification allows inexact division; this
     evaluator divides exactly);
   * sin, cos, exp, pow, exp2, log, log2, tan, atan2 of f32 call the C library's
-    single-precision functions (sinf, ...), which are within the error bounds the
-    specification allows;
+    single-precision functions (sinf, ...), or, for a module created with
+    transcendentals="f64", the double-precision ones rounded to f32; both are within the
+    error bounds the specification allows;
   * AbstractFloat / AbstractInt literals and constant expressions built only from them are
     evaluated in float64 / int64 and converted (rounded to nearest) when they meet a
     concrete type or initialise a let/var (WGSL's concretisation rules);
@@ -121,6 +122,14 @@ class Parser:
             raise SyntaxError(f"expected {text!r}, got {tok.text!r} near token {self.i}")
         return tok
 
+    def expect_close(self):
+        """A template's closing '>' (the tokenizer reads '>>' in array<atomic<u32>> as one)."""
+        tok = self.peek()
+        if tok.text == ">>":
+            self.t[self.i] = Tok("op", ">")
+            return
+        self.expect(">")
+
     # types
     def parse_type(self):
         name = self.next().text
@@ -131,7 +140,7 @@ class Parser:
         if name in ("vec2", "vec3", "vec4"):
             self.expect("<")
             el = self.next().text
-            self.expect(">")
+            self.expect_close()
             return ("vec", int(name[3]), el)
         if name == "array":
             self.expect("<")
@@ -139,12 +148,12 @@ class Parser:
             count = None
             if self.accept(","):
                 count = self.parse_unary()  # not parse_expr: the closing '>' is not an operator here
-            self.expect(">")
+            self.expect_close()
             return ("array", el, count)
         if name == "atomic":
             self.expect("<")
             el = self.parse_type()
-            self.expect(">")
+            self.expect_close()
             return ("atomic", el)
         if name in self.structs:
             return ("struct", name)
@@ -409,6 +418,30 @@ class Val:
         return self.el in ("af", "ai")
 
 
+class SVal(dict):
+    """A struct value: field name -> Val (each over the lanes)."""
+
+    def __init__(self, name, fields):
+        super().__init__(fields)
+        self.name = name
+
+
+def sel(mask, new, old):
+    """new where mask, old elsewhere, for a Val or a struct value."""
+    if isinstance(new, SVal):
+        return SVal(new.name, {k: sel(mask, new[k], old[k]) for k in new})
+    return select_lanes(mask, new, old)
+
+
+def widen(v, L):
+    """A Val or struct value broadcast to L lanes."""
+    if isinstance(v, SVal):
+        return SVal(v.name, {k: widen(x, L) for k, x in v.items()})
+    if v.v.shape[0] != L:
+        return Val(v.el, v.n, np.broadcast_to(v.v, (L,) + v.v.shape[1:]).copy())
+    return v
+
+
 def _libm():
     lib = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
     fns = {}
@@ -550,10 +583,6 @@ SWZ.update({c: i for i, c in enumerate("rgba")})
 
 # ---------------------------------------------------------------- interpreter --------------
 
-class ReturnSignal(Exception):
-    pass
-
-
 class Frame:
     def __init__(self, lanes):
         self.alive = np.ones(lanes, bool)
@@ -570,8 +599,9 @@ class Frame:
 class Program:
     """A parsed WGSL module with storage bindings; run() dispatches an entry point."""
 
-    def __init__(self, src: str):
+    def __init__(self, src: str, transcendentals: str = "libm"):
         self.p = Parser(src).parse_module()
+        self.transcendentals = transcendentals
         self.bindings = {}  # global name -> numpy array (storage) or dict of Val (uniform struct)
         self.uniform_vals = {}
 
@@ -648,13 +678,13 @@ class Program:
                 v = self.zero(ty)
             else:
                 v = self.eval(init, fr, mask)
-                if ty is not None:
+                if isinstance(v, SVal):
+                    pass
+                elif ty is not None:
                     v = convert(v, ty[1] if ty[0] == "scalar" else ty[2])
                 else:
                     v = concretize(v)
-            if v.v.shape[0] != self.L:
-                v = Val(v.el, v.n, np.broadcast_to(v.v, (self.L,) + v.v.shape[1:]).copy())
-            fr.scopes[-1][name] = v
+            fr.scopes[-1][name] = widen(v, self.L)
         elif k == "assign":
             lhs, op, rhs = s.a, s.b, s.c
             val = self.eval(rhs, fr, mask)
@@ -705,15 +735,33 @@ class Program:
         elif k == "return":
             if s.a is not None:
                 v = self.eval(s.a, fr, mask)
-                if fr.ret is None:
-                    fr.ret = Val(v.el, v.n, np.zeros((self.L,) + v.v.shape[1:], v.v.dtype))
-                v = convert(v, fr.ret.el) if v.el != fr.ret.el else v
-                fr.ret = select_lanes(mask, Val(v.el, v.n, np.broadcast_to(v.v, fr.ret.v.shape)), fr.ret)
+                if isinstance(v, SVal):
+                    v = widen(v, self.L)
+                    fr.ret = v if fr.ret is None else sel(mask, v, fr.ret)
+                else:
+                    if fr.ret is None:
+                        fr.ret = Val(v.el, v.n, np.zeros((self.L,) + v.v.shape[1:], v.v.dtype))
+                    v = convert(v, fr.ret.el) if v.el != fr.ret.el else v
+                    fr.ret = select_lanes(mask, Val(v.el, v.n, np.broadcast_to(v.v, fr.ret.v.shape)), fr.ret)
             fr.alive = fr.alive & ~mask
         else:
             raise SyntaxError(k)
 
+    def struct_layout(self, name):
+        """(field, element, width, float offset) of a struct of scalars and vectors, packed
+        as a storage array of vec4 / f32 fields lays them out."""
+        out, off = [], 0
+        for fname, fty in self.p.structs[name]:
+            n = fty[1] if fty[0] == "vec" else 0
+            el = fty[2] if n else fty[1]
+            out.append((fname, el, n, off))
+            off += n or 1
+        return out
+
     def zero(self, ty):
+        if ty[0] == "struct":
+            return SVal(ty[1], {f: Val(el, n, np.zeros((self.L, n) if n else self.L, DT[el]))
+                                for f, el, n, _ in self.struct_layout(ty[1])})
         if ty[0] == "scalar":
             return Val(ty[1], 0, np.zeros(self.L, DT[ty[1]]))
         if ty[0] == "vec":
@@ -730,6 +778,9 @@ class Program:
             if scope is None:
                 raise NameError(lhs.a)
             old = scope[lhs.a]
+            if isinstance(old, SVal):
+                scope[lhs.a] = sel(mask, widen(val, self.L), old)
+                return
             val = convert(val, old.el) if val.el != old.el else val
             if val.n == 0 and old.n:
                 val = Val(val.el, old.n, np.broadcast_to(val.v[..., None], old.v.shape))
@@ -738,11 +789,29 @@ class Program:
             base = lhs.a
             scope = fr.lookup(base.a)
             old = scope[base.a]
+            if isinstance(old, SVal):  # struct field: s.f = ...
+                f = old[lhs.b]
+                val = convert(val, f.el) if val.el != f.el else val
+                if val.n == 0 and f.n:
+                    val = Val(val.el, f.n, np.broadcast_to(val.v[..., None], f.v.shape))
+                new = dict(old)
+                new[lhs.b] = select_lanes(mask, Val(f.el, f.n, np.broadcast_to(val.v, f.v.shape)), f)
+                scope[base.a] = SVal(old.name, new)
+                return
             comp = SWZ[lhs.b]
             val = convert(val, old.el) if val.el != old.el else val
             newv = old.v.copy()
             newv[:, comp] = np.where(mask, np.broadcast_to(val.v, (self.L,)), old.v[:, comp])
             scope[base.a] = Val(old.el, old.n, newv)
+        elif lhs.kind == "index" and isinstance(val, SVal):  # a struct into an array of structs
+            arr = self.bindings[lhs.a.a]
+            idx = self.eval(lhs.b, fr, mask)
+            ii = np.broadcast_to(idx.v.astype(np.int64), (self.L,))
+            if mask.any() and (ii[mask].min() < 0 or ii[mask].max() >= arr.shape[0]):
+                raise IndexError(f"store out of bounds in {lhs.a.a}")
+            for f, el, n, off in self.struct_layout(val.name):
+                fv = widen(val[f], self.L).v
+                arr[ii[mask], off:off + (n or 1)] = (fv[mask] if n else fv[mask][:, None]).astype(arr.dtype)
         elif lhs.kind == "index":
             arr, el, n = self.buffer(lhs.a)
             idx = self.eval(lhs.b, fr, mask)
@@ -769,6 +838,8 @@ class Program:
             ty = self.p.globals[name][1][1]
         if ty[0] == "atomic":
             ty = ty[1]
+        if ty[0] == "struct":
+            return arr, ("struct", ty[1]), 0
         return arr, (ty[1] if ty[0] == "scalar" else ty[2]), (ty[1] if ty[0] == "vec" else 0)
 
     # expressions
@@ -807,6 +878,10 @@ class Program:
                 return Val(el, n, arr[self.wg_of_lane, ii])
             if mask.any() and (ii[mask].min() < 0 or ii[mask].max() >= arr.shape[0]):
                 raise IndexError(f"read out of bounds in {e.a.a}")
+            if isinstance(el, tuple):  # array of structs: one row of floats per element
+                rows = arr[ii]
+                return SVal(el[1], {f: Val(fe, fn, rows[:, off:off + fn] if fn else rows[:, off])
+                                    for f, fe, fn, off in self.struct_layout(el[1])})
             return Val(el, n, arr[ii])
         if k == "un":
             if e.a == "&":
@@ -851,10 +926,9 @@ class Program:
             sub = Frame(self.L)
             sub.alive = mask.copy()
             for (pname, pty, _), a in zip(f.params, args):
-                a = convert(a, pty[1] if pty[0] == "scalar" else pty[2])
-                if a.v.shape[0] != self.L:
-                    a = Val(a.el, a.n, np.broadcast_to(a.v, (self.L,) + a.v.shape[1:]).copy())
-                sub.scopes[0][pname] = a
+                if not isinstance(a, SVal):
+                    a = convert(a, pty[1] if pty[0] == "scalar" else pty[2])
+                sub.scopes[0][pname] = widen(a, self.L)
             self.exec_block(f.body, sub, mask)
             return sub.ret
         return self.builtin(name, argn, fr, mask)
@@ -909,6 +983,8 @@ class Program:
             return mk(np.sqrt(args[0].v))
         if name == "floor":
             return mk(np.floor(args[0].v))
+        if name == "round":  # halfway cases to the even integer
+            return mk(np.rint(args[0].v))
         if name == "ceil":
             return mk(np.ceil(args[0].v))
         if name == "fract":
@@ -968,6 +1044,10 @@ class Program:
             if el == "f16":
                 raise NotImplementedError("f16 transcendentals")
             vs, n = bc(*args)
+            if self.transcendentals == "f64":
+                fn = {"pow": math.pow, "atan2": math.atan2, "exp2": lambda x: 2.0 ** x}.get(name) or getattr(math, name)
+                ws = np.broadcast_arrays(*[np.asarray(v, np.float64) for v in vs])
+                return Val(el, n, np.vectorize(fn, otypes=[np.float64])(*ws).astype(np.float32))
             return Val(el, n, _map_f32(libf[name], *vs))
         raise NameError(f"builtin {name}")
 

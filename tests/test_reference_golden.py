@@ -6,11 +6,14 @@ text of src/sim/firex/shaders.ts:1-512 and pressureShaders.ts:1-161, evaluated o
 (tests/golden/reference_step.py), by tests/golden/make_reference_golden.py. Each case starts
 from the reference's reset or from a seeded developed state (motion, heat, fuel, products,
 deposited liquid) and runs 2-3 steps in one of the three pressure branches, with the engine's
-default parameters or a stated parameter set, dt = 1/60, 0 or 1/30.
+default parameters or a stated parameter set, dt = 1/60, 0 or 1/30; two cases run the SPH
+droplet passes (shaders.ts:514-825) with the jet and the spray nozzle, one of them switching
+the spray off before its last step.
 
-The oracle must reproduce every field after every step bit for bit: its f32 restatement
-performs the same IEEE operations in the same order, and both sides take sin / cos / exp /
-pow from the same C library. The GPU tests compare the CUDA path with the same fixtures
+The oracle must reproduce every field, the droplets and the integer liquid field after every
+step bit for bit: its f32 restatement performs the same IEEE operations in the same order, and
+both sides take sin / cos / exp / pow from the same C library (the droplet passes' sin, cos,
+tan and exp in double precision rounded to f32, on both sides). The GPU tests compare the CUDA path with the same fixtures
 within the tolerances that CUDA's own transcendentals require.
 """
 from __future__ import annotations
@@ -51,7 +54,7 @@ def start_sim(cls, case, **kw):
     m = META[case]
     dims = tuple(m["dims"])
     opts = make_options(pressure_iterations=m["P"], correction_iterations=m["R"], pressure_mode=BRANCH[m["branch"]],
-                        cinematic=m["cinematic"])
+                        cinematic=m["cinematic"], particle_count=m.get("droplets", 0))
     sim = cls(dims, opts, **kw)
     for name, value in m["parameters"].items():
         sim.set_parameter(name, value)
@@ -62,6 +65,12 @@ def start_sim(cls, case, **kw):
     return sim, dims
 
 
+def apply_changes(sim, case, i):
+    """Parameter changes the case makes before step i (e.g. the spray switched off)."""
+    for name, value in META[case].get("changes", {}).get(str(i), {}).items():
+        sim.set_parameter(name, value)
+
+
 @pytest.mark.parametrize("case", sorted(META))
 def test_oracle_reproduces_the_reference_step(case):
     m = META[case]
@@ -69,12 +78,17 @@ def test_oracle_reproduces_the_reference_step(case):
     for f in ("flow", "species", "pressure", "liquid"):
         assert np.array_equal(o.read(f), reshape(f, DATA[f"{case}/in/{f}"], dims)), f"start state {f}"
     for i, dt in enumerate(m["dts"]):
+        apply_changes(o, case, i)
         o.step(1, dt)
-        for f in FIELDS:
+        for f in FIELDS + ("liquid",):
             ref = reshape(f, DATA[f"{case}/step{i}/{f}"], dims)
             got = o.read(f)
             assert np.array_equal(got, ref), (f"{case} step {i} {f}: {int((got != ref).sum())} cells differ, "
                                               f"max abs {float(np.abs(got.astype(np.float64) - ref).max())}")
+        if m.get("droplets"):
+            ref = DATA[f"{case}/step{i}/particles"]
+            got = o.read_particles().reshape(ref.shape)
+            assert np.array_equal(got, ref), f"{case} step {i} droplets: {int((got != ref).sum())} values differ"
     st = o.state
     fin = m["final"]
     assert st["frame_index"] == fin["frame_index"]
@@ -91,3 +105,6 @@ def test_fixture_cases_cover_every_branch_and_start():
     assert branches == {"A", "B", "C"} and starts == {"reset", "developed"}
     assert 0.0 in dts and len(dts) >= 3
     assert any(m["parameters"] for m in META.values()) and any(m["cinematic"] == 0 for m in META.values())
+    # droplets with both nozzles, and the spray switched off mid-run
+    nozzles = {m["parameters"].get("nozzleType") for m in META.values() if m.get("droplets")}
+    assert nozzles == {0, 1} and any(m.get("changes") for m in META.values() if m.get("droplets"))
