@@ -20,8 +20,8 @@
 // [lo, hi] of |x| where Markstein's correction step (fx_div_checked) reproduces IEEE
 // x / d; ok = 1 once the engine has checked that on the device for every float x.
 struct __align__(16) FxDivc {  // one 16-byte load brings d, rcp, lo and hi
-    float d, rcp, lo, hi;
-    int ok, pad[3];
+    float d, rcp, lo, hi;         // lo = +inf when the checked path is not enabled
+    int ok, pad[3];               // host record of the device check
 };
 enum FxDivSlot {
     DIVC_SIX = 0,        // the 6-neighbour averages (shaders.ts:177-186)

@@ -527,6 +527,8 @@ struct firex_sim {
             // dt may change every call: its divisor keeps the IEEE division rather than
             // paying the device check per new value
             c.ok = (k != DIVC_DT && c.d > 0.0f && c.d < 1073741824.0f && fast_division_ok(device, c.d, c.rcp, c.lo, c.hi)) ? 1 : 0;
+            // not enabled: an empty fast range sends every x to the IEEE division (fx_divc)
+            if (!c.ok) c.lo = INFINITY;
         }
         dirty = true;
     }

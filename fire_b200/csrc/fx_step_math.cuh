@@ -38,10 +38,12 @@ FXD float fx_div_range(float x, float d, float rcp, float lo, float hi) {
 
 FXD float fx_div_by_const(float x, float d, float rcp) { return fx_div_range(x, d, rcp, 1.2621774483536189e-29f, 3.402823466e38f); }
 
-// x / c.d, by the checked constant-divisor path when the engine enabled it.
+// x / c.d, by the checked constant-divisor path when the engine enabled it. A divisor the
+// engine did not enable carries lo = +inf, so every x takes the IEEE division of
+// fx_div_range's rare path (zeros keep their sign): one 16-byte load, no flag.
 FXD float fx_divc(float x, const FxDivc& c) {
     const float4 v = __ldg(reinterpret_cast<const float4*>(&c));  // d, rcp, lo, hi
-    return __ldg(&c.ok) ? fx_div_range(x, v.x, v.y, v.z, v.w) : __fdiv_rn(x, v.x);
+    return fx_div_range(x, v.x, v.y, v.z, v.w);
 }
 
 // smoothstep with its constant denominator e1 - e0 held in c.
