@@ -56,6 +56,9 @@ JACOBI_RESIDENT = 4
 STAGING_AUTO = 0
 STAGING_CPASYNC = 1
 STAGING_TMA = 2
+PROJECT_AUTO = 0
+PROJECT_FUSED = 1
+PROJECT_SEPARATE = 2
 
 VALUE_NUMBER = 0
 VALUE_BOOLEAN = 1
@@ -152,7 +155,8 @@ class Diagnostics(C.Structure):
         ("jacobi_variant", C.c_int32),
         ("jacobi_staging", C.c_int32),
         ("simulate_by", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("project_fused", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -211,8 +215,8 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_batch_set_jacobi": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
         "firex_set_staging": (C.c_int, [vp, C.c_int32]),
         "firex_batch_set_staging": (C.c_int, [vp, C.c_int32]),
-        "firex_set_tiles": (C.c_int, [vp, C.c_int32]),
-        "firex_batch_set_tiles": (C.c_int, [vp, C.c_int32]),
+        "firex_set_tiles": (C.c_int, [vp, C.c_int32, C.c_int32]),
+        "firex_batch_set_tiles": (C.c_int, [vp, C.c_int32, C.c_int32]),
         "firex_batch_create": (C.c_int, [C.POINTER(vp)]),
         "firex_batch_destroy": (C.c_int, [vp]),
         "firex_batch_add": (C.c_int, [vp, vp]),

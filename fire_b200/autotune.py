@@ -8,8 +8,9 @@ ordinary steps of the run: the trajectory is the same whichever candidate ran th
 candidates are the resident kernel in each box variant that fits, the single-sweep kernels
 (unblocked, and z-marching with 8, 16 or 32 planes per CTA) and the two-sweep pass with 16-,
 32- or 64-plane chunks, its planes staged by TMA or by cp.async. With the fastest Jacobi
-applied, the source pass's bricks (32 x 4 x 2, 32 x 2 x 4, 32 x 8 x 1 cells) are timed the
-same way; every shape computes each cell with the same operations. The winner is applied
+applied, the source pass's bricks (32 x 4 x 2, 32 x 2 x 4, 32 x 8 x 1 cells), each with the
+primary projection fused with the residual divergence or run as two passes, are timed the same
+way; every choice computes each cell with the same operations. The winner is applied
 (set_jacobi, set_staging, set_tiles) and remembered per workload signature (grid sizes,
 sweep counts, precision, pressure branch), optionally in a JSON file so that a later process
 starts tuned.
@@ -34,9 +35,10 @@ class Candidate:
     zchunk: int = 0
     staging: int = A.STAGING_AUTO  # two-sweep pass: TMA (FP32 pressure) or cp.async
     simulate_by: int = 0           # source-pass bricks: 32 x by x (8 / by); 0 = default
+    project: int = A.PROJECT_AUTO  # primary projection fused with the residual divergence or not
 
     def as_list(self) -> list:
-        return [self.kernel, self.block, self.zchunk, self.staging, self.simulate_by]
+        return [self.kernel, self.block, self.zchunk, self.staging, self.simulate_by, self.project]
 
 
 def default_candidates() -> list:
@@ -108,7 +110,7 @@ class JacobiTuner:
     def apply(target, c: Candidate) -> None:
         target.set_jacobi(c.kernel, c.block, c.zchunk)
         target.set_staging(c.staging)
-        target.set_tiles(c.simulate_by)
+        target.set_tiles(c.simulate_by, c.project)
 
     def tune(self, target, dt: float = 1.0 / 60.0, force: bool = False) -> Candidate:
         """Times every Jacobi candidate on `target` (a FireXSim or FireXBatch) for warmup +
@@ -132,10 +134,11 @@ class JacobiTuner:
             return Candidate("auto")
         best = min(timings, key=timings.get)
         for by in SIMULATE_SHAPES:
-            c = Candidate(best.kernel, best.block, best.zchunk, best.staging, by)
-            self.apply(target, c)
-            target.step(self.warmup, dt)
-            timings[c] = self._time(target, dt)
+            for proj in (A.PROJECT_FUSED, A.PROJECT_SEPARATE):
+                c = Candidate(best.kernel, best.block, best.zchunk, best.staging, by, proj)
+                self.apply(target, c)
+                target.step(self.warmup, dt)
+                timings[c] = self._time(target, dt)
         best = min(timings, key=timings.get)
         self.apply(target, best)
         self.last_timings = {json.dumps(c.as_list()): ms for c, ms in timings.items()}

@@ -137,13 +137,14 @@ struct StepPlan {
     bool pack = false;        // a member packs its render volumes at the end of every step
     bool tma = false;         // the two-sweep pass stages its planes by TMA
     int simBy = FX_CELL_BY;   // source-pass bricks: 32 x simBy x (8 / simBy) cells
+    bool projDiv = true;      // the primary projection and the residual divergence in one pass
     bool res = false;         // every sweep of a phase in one resident launch
     int resVariant = 0;       // ... by this variant of the kernel
     int resSmem = 0;          // its dynamic shared memory per CTA
     int bricks[FX_NSHAPES] = {};
     auto key() const {
-        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, tma, simBy, res, resVariant,
-                        resSmem,
+        return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, tma, simBy, projDiv, res,
+                        resVariant, resSmem,
                         bricks[0],
                         bricks[1], bricks[2], bricks[3], bricks[4], bricks[5], bricks[6]);
     }
@@ -190,7 +191,12 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
     fx_launch_simulate(st, pl.storage, pl.simBy, B, pl.bricks[FX_SHAPE_CELL]);
     fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 0);
     enqueue_jacobi_phase(st, pl, B, 0);
-    fx_launch_project_div(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4]);
+    if (pl.projDiv) {
+        fx_launch_project_div(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4]);
+    } else {
+        fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 0);
+        fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 1);
+    }
     enqueue_jacobi_phase(st, pl, B, 1);
     fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 1);
     fx_launch_step_end(st, B);
@@ -381,6 +387,7 @@ struct firex_sim {
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;
     int staging = FIREX_STAGING_AUTO;  // how the two-sweep pass stages its planes
     int simBy = 0;                     // source-pass brick height (0: FX_CELL_BY)
+    int projFuse = FIREX_PROJECT_AUTO; // primary projection fused with the residual divergence?
 
     FxSimDev h{};           // host mirror of the device descriptor
     FxSimDev* d = nullptr;  // device descriptor
@@ -595,6 +602,7 @@ struct firex_batch {
     int jacobiKernel = FIREX_JACOBI_AUTO, jacobiK = 1, jacobiZc = 0;  // batch override (AUTO: first member's)
     int staging = FIREX_STAGING_AUTO;  // batch override of the members' staging (AUTO: first member's)
     int simBy = 0;                     // batch override of the source-pass bricks (0: first member's)
+    int projFuse = FIREX_PROJECT_AUTO; // batch override of the projection fusion (AUTO: first member's)
     int tableK = -1, tableZc = -1, tableZmZc = -1;  // launch shapes the prefix sums were built for
     int tableSimBy = -1;
     int tableRes = -1;                               // whether resident boxes were requested
@@ -731,6 +739,8 @@ struct firex_batch {
         p.zmZc = (kernel == FIREX_JACOBI_ZMARCH && zc > 0) ? zc : zm_chunk(zm32, zm16);
         const int by = this->simBy ? this->simBy : members[0]->simBy;
         p.simBy = by ? by : FX_CELL_BY;
+        const int pf = this->projFuse != FIREX_PROJECT_AUTO ? this->projFuse : members[0]->projFuse;
+        p.projDiv = pf != FIREX_PROJECT_SEPARATE;
         if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 2 + resForce : 0) ||
             tableWater != water_signature() || tableSimBy != p.simBy)
             fill_table(p.k, p.zc, p.zmZc, wantRes, resForce, p.simBy);
@@ -807,8 +817,15 @@ struct firex_batch {
         mark(FIREX_PASS_DIVERGENCE, 1);
         enqueue_jacobi_phase(stream, pl, d, 0);
         mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 0));
-        fx_launch_project_div(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4]);
-        mark(FIREX_PASS_PROJECT, 1);
+        if (pl.projDiv) {
+            fx_launch_project_div(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4]);
+            mark(FIREX_PASS_PROJECT, 1);
+        } else {
+            fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 0);
+            mark(FIREX_PASS_PROJECT, 1);
+            fx_launch_divergence(stream, d, pl.bricks[FX_SHAPE_ROW4], 1);
+            mark(FIREX_PASS_DIVERGENCE, 1);
+        }
         enqueue_jacobi_phase(stream, pl, d, 1);
         mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 1));
         fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 1);
@@ -879,7 +896,7 @@ struct firex_batch {
             if (!profiling) {
                 pendingLaunches[FIREX_PASS_OTHER] += pl.pack ? 4 : 3;
                 pendingLaunches[FIREX_PASS_SIMULATE] += 1;
-                pendingLaunches[FIREX_PASS_DIVERGENCE] += 1;
+                pendingLaunches[FIREX_PASS_DIVERGENCE] += pl.projDiv ? 1 : 2;
                 pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
                 pendingLaunches[FIREX_PASS_PROJECT] += 2;
                 pendingLaunches[FIREX_PASS_PARTICLES] += sph_launches(pl);
@@ -1620,12 +1637,14 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
     out->launches_per_step =
-        7 + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) + jacobi_phase_launches(p, 1);
+        (p.projDiv ? 7 : 8) + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) +
+        jacobi_phase_launches(p, 1);
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
     out->jacobi_variant = p.res ? p.resVariant : -1;
     out->jacobi_staging = p.tma ? FIREX_STAGING_TMA : (p.k == 2 ? FIREX_STAGING_CPASYNC : -1);
     out->simulate_by = p.simBy;
+    out->project_fused = p.projDiv ? 1 : 0;
     return FIREX_OK;
 }
 
@@ -1667,15 +1686,19 @@ int firex_batch_set_staging(firex_batch* b, int32_t staging) {
     return FIREX_OK;
 }
 
-int firex_set_tiles(firex_sim* s, int32_t simulate_by) {
-    if (!s || !sim_by_ok(simulate_by)) return FIREX_ERR_BAD_ARG;
+static bool proj_ok(int p) { return p >= FIREX_PROJECT_AUTO && p <= FIREX_PROJECT_SEPARATE; }
+
+int firex_set_tiles(firex_sim* s, int32_t simulate_by, int32_t project) {
+    if (!s || !sim_by_ok(simulate_by) || !proj_ok(project)) return FIREX_ERR_BAD_ARG;
     s->simBy = simulate_by;
+    s->projFuse = project;
     return FIREX_OK;
 }
 
-int firex_batch_set_tiles(firex_batch* b, int32_t simulate_by) {
-    if (!b || !sim_by_ok(simulate_by)) return FIREX_ERR_BAD_ARG;
+int firex_batch_set_tiles(firex_batch* b, int32_t simulate_by, int32_t project) {
+    if (!b || !sim_by_ok(simulate_by) || !proj_ok(project)) return FIREX_ERR_BAD_ARG;
     b->simBy = simulate_by;
+    b->projFuse = project;
     return FIREX_OK;
 }
 

@@ -47,8 +47,9 @@
 // Words of FxSimDev::sync after the error word [2], set from the host (firex_set_wait_limit,
 // firex_test_hold_face) and zero by default:
 //   [3] polls of a neighbour's flag before a wait gives up (0: FX_RES_SPIN_LIMIT);
-//   [4] box + 1 that does not publish its faces of sweep [5] (0: every box publishes) — a
-//       flag that nothing sets, so the neighbours' bounded waits expire (test of the error path).
+//   [4] box + 1 that stops publishing its faces from sweep [5] on (0: every box publishes) —
+//       a flag that nothing sets (the flags only grow, so a single withheld sweep would only
+//       delay the neighbours), so their bounded waits expire (test of the error path).
 #define FX_SYNC_SPIN 3
 #define FX_SYNC_HOLD_BOX 4
 #define FX_SYNC_HOLD_SWEEP 5
@@ -95,7 +96,7 @@ FXD unsigned fx_res_spin_limit(const unsigned* err) {
 // Publishes box `me`'s faces of sweep s (flag = s + 1, release), unless the host holds them back.
 FXD void fx_res_publish(unsigned* flags, int me, unsigned s, const unsigned* err) {
     const unsigned* sync = fx_res_sync(err);
-    if (sync[FX_SYNC_HOLD_BOX] == (unsigned)me + 1 && sync[FX_SYNC_HOLD_SWEEP] == s) return;
+    if (sync[FX_SYNC_HOLD_BOX] == (unsigned)me + 1 && s >= sync[FX_SYNC_HOLD_SWEEP]) return;
     fx_st_release_u32(flags + me, s + 1);
 }
 

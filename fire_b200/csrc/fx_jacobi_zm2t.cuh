@@ -36,6 +36,9 @@
 #define FX_T2_PSLOT 1376                // floats per pressure slot: 5440 B padded to 43 x 128 B
 #define FX_T2_DSLOT (FX_Z2_COLS * FX_T2_DBOX_Y)  // 1280 floats = 40 x 128 B
 #define FX_T2_WAIT_LIMIT (1u << 22)
+#ifndef FX_T2_ONE_WAITER
+#define FX_T2_ONE_WAITER 1
+#endif
 
 // Tensor maps of a simulation (FxSimDev::tmap): pressure pair, correction pair, divergence.
 enum { FX_TM_P0 = 0, FX_TM_P1 = 1, FX_TM_C0 = 2, FX_TM_C1 = 3, FX_TM_DIV = 4, FX_TM_COUNT = 5 };
@@ -128,9 +131,13 @@ FXD bool fx_zm2t_tile(const FxSimDev& S, const CUtensorMap* tmP, float* __restri
         if (!ZERO_IN) fx_tma_load3(sm.p[slot], tmP, x0 - 4, y0 - 2, qc, &sm.bar[slot]);
         fx_tma_load3(sm.d[slot], tmD, x0 - 4, y0 - 1, qc, &sm.bar[slot]);
     };
-    // waits for the plane in `slot`; on expiry every thread learns it at the next barrier
+    // waits for the plane in `slot`; on expiry every thread learns it at the next barrier.
+    // With FX_T2_ONE_WAITER one thread polls the barrier and the step's CTA barrier that
+    // follows passes the landed plane on to the others (the TMA writes the waiting thread
+    // observed are ordered before everything after the CTA barrier); else every thread polls.
     auto wait = [&](int slot) {
-        if (!fx_mbar_wait(&sm.bar[slot], (phases >> slot) & 1u, FX_T2_WAIT_LIMIT)) sm.err = 1;
+        if (!FX_T2_ONE_WAITER || t == 0)
+            if (!fx_mbar_wait(&sm.bar[slot], (phases >> slot) & 1u, FX_T2_WAIT_LIMIT)) sm.err = 1;
         phases ^= 1u << slot;
     };
     if (t == 0) {

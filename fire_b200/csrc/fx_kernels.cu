@@ -348,6 +348,9 @@ __global__ void __launch_bounds__(256, 8) fxk_project(const FxBatchDev* __restri
 //                          top row (the top row copies the projected row below).
 // The extra loads (one component of the flow and one pressure value per neighbour) hit
 // L1/L2: the rows and planes behind were read by the warps and CTAs before.
+#ifndef FX_PROJDIV_MINB
+#define FX_PROJDIV_MINB 6  // CTAs per SM the fused projection's registers are budgeted for
+#endif
 template <typename PT>
 struct ProjSrc {
     const float4* __restrict__ flowIn;
@@ -382,7 +385,7 @@ struct ProjSrc {
 };
 
 template <typename PT>
-__global__ void __launch_bounds__(256, 4) fxk_project_div(const FxBatchDev* __restrict__ B) {
+__global__ void __launch_bounds__(256, FX_PROJDIV_MINB) fxk_project_div(const FxBatchDev* __restrict__ B) {
     fx_for_bricks<FX_SHAPE_ROW4>(B, [&](const FxSimDev& S, int b) {
         const Lane4 r = fx_lane4(S, b);
         if (r.n <= 0) return;  // warp-uniform
@@ -394,14 +397,17 @@ __global__ void __launch_bounds__(256, 4) fxk_project_div(const FxBatchDev* __re
         const int X = S.X, XY = S.X * S.Y;
         int xs[4], ys[4], zs[4];
         fx_lane4_coords(S, r, xs, ys, zs);
-        float4 o[4];
-        float vb[4], wk[4];
+        // u of the cell before lane 0's first cell (another warp's or brick's cell)
+        float prevU = (lane == 0 && xs[0] > 0) ? src.u(r.c0 - 1, xs[0] - 1, ys[0]) : 0.0f;
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            o[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            vb[i] = wk[i] = 0.0f;
-            if (lane + 32 * i < r.n) {
-                const int c = r.c0 + 32 * i;
+            // each of the lane's cells is finished in its own iteration: only the u that the
+            // next group's first lane needs is carried (registers for more CTAs per SM)
+            const bool valid = lane + 32 * i < r.n;
+            const int c = r.c0 + 32 * i;
+            float4 q = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            float vb = 0.0f, wk = 0.0f;
+            if (valid) {
                 const int cs = (ys[i] == S.Y - 1) ? c - X : c;  // top row: the projected row below
                 const float4 f = __ldg(src.flowIn + c);
                 const float4 s = (cs == c) ? f : __ldg(src.flowIn + cs);
@@ -415,27 +421,19 @@ __global__ void __launch_bounds__(256, 4) fxk_project_div(const FxBatchDev* __re
                 const float gx = (px - pc) * src.m.x;
                 const float gy = (pt - pc) * src.m.y;
                 const float gz = (pf - pc) * src.m.z;
-                float4 q = make_float4(s.x - gx, s.y - gy, s.z - gz, f.w);
+                q = make_float4(s.x - gx, s.y - gy, s.z - gz, f.w);
                 if (xs[i] == 0 || xs[i] == X - 1) q.x = 0.0f;
                 if (zs[i] == 0 || zs[i] == S.Z - 1) q.z = 0.0f;
                 if (ys[i] == 0) q.y = 0.0f;
                 if (ys[i] == S.Y - 1) q.y = fx_max(0.0f, q.y);
                 flowOut[c] = q;
-                o[i] = q;
-                vb[i] = ys[i] > 0 ? src.v(c - X, ys[i] - 1) : q.y;
-                wk[i] = zs[i] > 0 ? src.w(c - XY, ys[i], zs[i] - 1) : q.z;
+                vb = ys[i] > 0 ? src.v(c - X, ys[i] - 1) : q.y;
+                wk = zs[i] > 0 ? src.w(c - XY, ys[i], zs[i] - 1) : q.z;
             }
-        }
-        // u of the cell before lane 0's first cell (another warp's or brick's cell)
-        float prevU = (lane == 0 && r.n > 0 && xs[0] > 0) ? src.u(r.c0 - 1, xs[0] - 1, ys[0]) : 0.0f;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const float fromLeft = __shfl_up_sync(0xffffffffu, o[i].x, 1);
-            const float ul = xs[i] == 0 ? o[i].x : (lane > 0 ? fromLeft : prevU);
-            prevU = __shfl_sync(0xffffffffu, o[i].x, 31);
-            if (lane + 32 * i < r.n)
-                S.div[r.c0 + 32 * i] =
-                    (o[i].x - ul) * src.m.x + (o[i].y - vb[i]) * src.m.y + (o[i].z - wk[i]) * src.m.z;
+            const float fromLeft = __shfl_up_sync(0xffffffffu, q.x, 1);
+            const float ul = xs[i] == 0 ? q.x : (lane > 0 ? fromLeft : prevU);
+            prevU = __shfl_sync(0xffffffffu, q.x, 31);
+            if (valid) S.div[c] = (q.x - ul) * src.m.x + (q.y - vb) * src.m.y + (q.z - wk) * src.m.z;
         }
     });
 }

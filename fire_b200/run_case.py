@@ -3,7 +3,8 @@
     python -m fire_b200.run_case X Y Z [--steps N] [--jacobi auto|unblocked|zmarch|fused|resident]
                                        [--block K] [--zchunk ZC] [--pressure auto|warm_f32|f16|cold_f32]
                                        [--mixed] [--iters P R] [--profile] [--time N]
-                                       [--staging auto|cpasync]
+                                       [--staging auto|cpasync] [--project auto|fused|separate]
+                                       [--simulate-by 2|4|8]
 
 A sphere emitter near the floor (radius X/9), seeded velocity noise and emission jitter,
 dt = 1/60. Used as the command under profilers (one process, one GPU, small cases).
@@ -36,6 +37,9 @@ def main() -> None:
     ap.add_argument("--time", type=int, default=0, help="then time this many steps (graph replay)")
     ap.add_argument("--staging", default="auto", choices=["auto", "cpasync"],
                     help="plane staging of the two-sweep pass (auto: TMA with FP32 pressure)")
+    ap.add_argument("--project", default="auto", choices=["auto", "fused", "separate"],
+                    help="primary projection and residual divergence in one pass or two")
+    ap.add_argument("--simulate-by", type=int, default=0, choices=[0, 2, 4, 8], help="source-pass brick height")
     a = ap.parse_args()
     X, Y, Z = a.dims
     opts = make_options(pressure_iterations=a.iters[0], correction_iterations=a.iters[1], seed=1, velocity_noise=0.05,
@@ -45,6 +49,7 @@ def main() -> None:
     s = FireXSim((X, Y, Z), opts)
     s.set_jacobi(a.jacobi, a.block, a.zchunk)
     s.set_staging(A.STAGING_CPASYNC if a.staging == "cpasync" else A.STAGING_AUTO)
+    s.set_tiles(a.simulate_by, {"auto": A.PROJECT_AUTO, "fused": A.PROJECT_FUSED, "separate": A.PROJECT_SEPARATE}[a.project])
     if a.profile:
         s.set_profiling(True)
         s.pass_times()

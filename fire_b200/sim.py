@@ -29,11 +29,13 @@ class FireXError(RuntimeError):
 
 
 def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
-    """Loads the CUDA library (once). Raises if it is missing: there is no fallback."""
+    """Loads the CUDA library (once): `path`, else the FIREX_LIBRARY environment variable (a
+    build of the same sources with other compile-time choices), else the in-tree build.
+    Raises if it is missing: there is no fallback."""
     global _LIB
     if _LIB is not None and path is None:
         return _LIB
-    p = Path(path) if path else LIB_PATH
+    p = Path(path) if path else Path(os.environ.get("FIREX_LIBRARY") or LIB_PATH)
     if not p.exists():
         raise FileNotFoundError(
             f"{p} is missing: build it with `python -m fire_b200.build` (no CPU fallback exists)")
@@ -283,8 +285,8 @@ class FireXSim(_Handle):
         self._check(self._lib.firex_set_wait_limit(self._h, int(polls)))
 
     def test_hold_face(self, box: int, sweep: int) -> None:
-        """Test hook: box `box` of the resident Jacobi withholds its faces of sweep `sweep`
-        (box < 0 clears it), so that its neighbours' bounded waits expire."""
+        """Test hook: box `box` of the resident Jacobi stops publishing its faces from sweep
+        `sweep` on (box < 0 clears it), so that its neighbours' bounded waits expire."""
         self._check(self._lib.firex_test_hold_face(self._h, int(box), int(sweep)))
 
     def set_jacobi(self, kernel, block: int = 0, zchunk: int = 0) -> None:
@@ -298,10 +300,11 @@ class FireXSim(_Handle):
         FP32) or A.STAGING_CPASYNC."""
         self._check(self._lib.firex_set_staging(self._h, int(staging)))
 
-    def set_tiles(self, simulate_by: int) -> None:
+    def set_tiles(self, simulate_by: int, project: int = 0) -> None:
         """Brick shape of the source pass: 32 x simulate_by x (8 / simulate_by) cells (2, 4, 8;
-        0: default)."""
-        self._check(self._lib.firex_set_tiles(self._h, int(simulate_by)))
+        0: default); `project`: A.PROJECT_FUSED / A.PROJECT_SEPARATE primary projection and
+        residual divergence (A.PROJECT_AUTO: fused)."""
+        self._check(self._lib.firex_set_tiles(self._h, int(simulate_by), int(project)))
 
     @property
     def diagnostics(self) -> dict:
@@ -378,8 +381,8 @@ class FireXBatch:
     def set_staging(self, staging: int) -> None:
         self._check(self._lib.firex_batch_set_staging(self._h, int(staging)))
 
-    def set_tiles(self, simulate_by: int) -> None:
-        self._check(self._lib.firex_batch_set_tiles(self._h, int(simulate_by)))
+    def set_tiles(self, simulate_by: int, project: int = 0) -> None:
+        self._check(self._lib.firex_batch_set_tiles(self._h, int(simulate_by), int(project)))
 
     def sync(self) -> None:
         self._check(self._lib.firex_batch_sync(self._h))

@@ -235,8 +235,8 @@ int firex_divergence_norm_noalloc(const void* flow, const int32_t dims[3], const
 int firex_set_wait_limit(firex_sim* sim, uint32_t polls);
 
 /* Test hook for the error path above (no reference counterpart): from the next step on, box
- * `box` of the resident Jacobi does not publish its faces of sweep `sweep` (in either phase),
- * a flag that nothing sets, so its neighbours' bounded waits expire. box < 0 clears it. */
+ * `box` of the resident Jacobi stops publishing its faces from sweep `sweep` on (in either
+ * phase), a flag that nothing sets, so its neighbours' bounded waits expire. box < 0 clears it. */
 int firex_test_hold_face(firex_sim* sim, int32_t box, int32_t sweep);
 
 /* Counters that decide ping-pong parity and time (FireXEngine.ts:396-409). */
@@ -361,12 +361,18 @@ int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, in
 int firex_set_staging(firex_sim* sim, int32_t staging);
 int firex_batch_set_staging(firex_batch* batch, int32_t staging);
 
-/* Brick shape of the source pass (simulate, shaders.ts:151-342): one thread per cell of a
- * 32 x simulate_by x (8 / simulate_by) brick, simulate_by = 2, 4 (the default) or 8; 0 restores
- * the default. The shapes give identical results; fire_b200/autotune.py times them. A batch's
- * own setting overrides its members' (0: the first member's). */
-int firex_set_tiles(firex_sim* sim, int32_t simulate_by);
-int firex_batch_set_tiles(firex_batch* batch, int32_t simulate_by);
+/* Launch shapes of the passes around the Jacobi. simulate_by: the source pass (simulate,
+ * shaders.ts:151-342) runs one thread per cell of a 32 x simulate_by x (8 / simulate_by) brick,
+ * simulate_by = 2, 4 (the default) or 8; 0 restores the default. project: the primary
+ * projection and the divergence of its result (the residual's right-hand side,
+ * FireXEngine.ts:2256-2257) run as one fused pass (FUSED) or as two (SEPARATE); AUTO = FUSED.
+ * Every choice gives identical results; fire_b200/autotune.py times them. A batch's own
+ * setting overrides its members' (0 / AUTO: the first member's). */
+#define FIREX_PROJECT_AUTO 0
+#define FIREX_PROJECT_FUSED 1
+#define FIREX_PROJECT_SEPARATE 2
+int firex_set_tiles(firex_sim* sim, int32_t simulate_by, int32_t project);
+int firex_batch_set_tiles(firex_batch* batch, int32_t simulate_by, int32_t project);
 
 /* What the engine chose for the most recent step of the simulation (or its batch). */
 typedef struct firex_diagnostics {
@@ -379,7 +385,8 @@ typedef struct firex_diagnostics {
     int32_t jacobi_variant;   /* RESIDENT: the box variant (0-3) it ran; else -1 */
     int32_t jacobi_staging;   /* two-sweep pass: FIREX_STAGING_TMA or _CPASYNC it ran; else -1 */
     int32_t simulate_by;      /* source-pass bricks of 32 x simulate_by x (8 / simulate_by) cells */
-    int32_t reserved[7];
+    int32_t project_fused;    /* 1: the primary projection and the residual divergence ran as one pass */
+    int32_t reserved[6];
 } firex_diagnostics;
 int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
 

@@ -28,8 +28,8 @@ class _Stub:
     def set_staging(self, staging):
         self.applied.append(("staging", staging))
 
-    def set_tiles(self, simulate_by):
-        self.applied.append(("tiles", simulate_by))
+    def set_tiles(self, simulate_by, project=0):
+        self.applied.append(("tiles", simulate_by, project))
 
     def step(self, *a):
         raise AssertionError("a cached workload must not step")
@@ -56,12 +56,13 @@ def test_cached_choice_is_applied_without_stepping(tmp_path):
     path.write_text(json.dumps({signature(stub): {"choice": ["zmarch", 0, 16], "ms_per_step": 1.0}}))
     t = JacobiTuner(cache_path=path)
     assert t.tune(stub) == Candidate("zmarch", 0, 16)
-    assert stub.applied == [("zmarch", 0, 16), ("staging", A.STAGING_AUTO), ("tiles", 0)]
+    assert stub.applied == [("zmarch", 0, 16), ("staging", A.STAGING_AUTO), ("tiles", 0, A.PROJECT_AUTO)]
     # a choice with staging and brick shape (the current cache format)
-    path.write_text(json.dumps({signature(stub): {"choice": ["fused", 2, 32, A.STAGING_CPASYNC, 8]}}))
+    path.write_text(json.dumps({signature(stub): {"choice": ["fused", 2, 32, A.STAGING_CPASYNC, 8,
+                                                            A.PROJECT_SEPARATE]}}))
     stub.applied.clear()
-    assert JacobiTuner(cache_path=path).tune(stub) == Candidate("fused", 2, 32, A.STAGING_CPASYNC, 8)
-    assert stub.applied == [("fused", 2, 32), ("staging", A.STAGING_CPASYNC), ("tiles", 8)]
+    assert JacobiTuner(cache_path=path).tune(stub) == Candidate("fused", 2, 32, A.STAGING_CPASYNC, 8, A.PROJECT_SEPARATE)
+    assert stub.applied == [("fused", 2, 32), ("staging", A.STAGING_CPASYNC), ("tiles", 8, A.PROJECT_SEPARATE)]
 
 
 @pytest.mark.gpu
@@ -112,20 +113,24 @@ def test_tuning_a_batch():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("by", [2, 8])
-def test_simulate_brick_shapes_are_bit_identical(by):
-    """The source pass's brick shapes the tuner chooses among (32 x by x 8/by cells) compute
-    every cell with the same operations: identical fields, on grids that end inside bricks."""
+@pytest.mark.parametrize("by,proj", [(2, A.PROJECT_FUSED), (8, A.PROJECT_SEPARATE), (4, A.PROJECT_SEPARATE)])
+def test_launch_shapes_are_bit_identical(by, proj):
+    """The source pass's brick shapes (32 x by x 8/by cells) and the fused or separate primary
+    projection + residual divergence, among which the tuner chooses, compute every cell with
+    the same operations: identical fields, on grids that end inside bricks."""
     from fire_b200.sim import FireXSim
 
     for dims in ((36, 44, 28), (100, 20, 12)):
-        opts = sphere_options(dims, P=6, R=6)
-        a, b = FireXSim(dims, opts), FireXSim(dims, opts)
-        b.set_tiles(by)
-        a.step(3, DT)
-        b.step(3, DT)
-        assert a.diagnostics["simulate_by"] == 4 and b.diagnostics["simulate_by"] == by
-        for f in ("flow", "species", "pressure", "divergence", "correction", "reaction"):
-            assert np.array_equal(a.read(f), b.read(f)), (dims, f)
-        a.close()
-        b.close()
+        for mode in (A.PRESSURE_WARM_F32, A.PRESSURE_F16):
+            opts = sphere_options(dims, P=6, R=6, pressure_mode=mode)
+            a, b = FireXSim(dims, opts), FireXSim(dims, opts)
+            b.set_tiles(by, proj)
+            a.step(3, DT)
+            b.step(3, DT)
+            assert a.diagnostics["simulate_by"] == 4 and b.diagnostics["simulate_by"] == by
+            assert a.diagnostics["project_fused"] == 1
+            assert b.diagnostics["project_fused"] == (proj != A.PROJECT_SEPARATE)
+            for f in ("flow", "species", "pressure", "divergence", "correction", "reaction"):
+                assert np.array_equal(a.read(f), b.read(f)), (dims, mode, f)
+            a.close()
+            b.close()

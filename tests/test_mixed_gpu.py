@@ -90,11 +90,14 @@ def test_mixed_step_divergence_vs_fp64(dims, P, R, warm):
     assert e16 <= REL_DIV_F16_PRESSURE, e16
     # FP16 species: the FP16 input (the FP64 state rounded on write) carried through one
     # step plus the rounding of the stored result, each within an FP16 ULP of the largest
-    # species value (2^-10 relative); the FP32 fields move only by what the species change
-    # in the source terms
+    # species value (2^-10 relative). The FP32 fields keep the FP32 step's own distance from
+    # FP64 (measured on B200: velocity, pressure and correction identical to the FP32 run's);
+    # temperature moves by what the FP16 species change in the heat release (4.5e-5 of the
+    # largest temperature measured)
     assert fmx["species_rel"] <= 2.0 ** -10 + f32["species_rel"], (fmx, f32)
-    for k in ("flow_uvw_rel", "flow_T_rel", "pressure_rel", "correction_rel"):
-        assert fmx[k] <= 1e-3, (k, fmx, f32)
+    for k in ("flow_uvw_rel", "pressure_rel", "correction_rel"):
+        assert fmx[k] <= 1.5 * f32[k] + 1e-6, (k, fmx, f32)
+    assert fmx["flow_T_rel"] <= 1e-4, (fmx, f32)
 
 
 def test_mixed_trajectory_divergence_norm_vs_fp64():

@@ -1,9 +1,9 @@
 """The resident Jacobi's bounded waits, made to expire on purpose.
 
 The resident kernel's CTAs wait on their neighbours' published faces with bounded polls
-(fx_jacobi_res.cuh). Here one box withholds its faces of one sweep (firex_test_hold_face: a
-flag that nothing sets) and the wait limit is short (firex_set_wait_limit): the neighbours'
-waits expire, each CTA sets the simulation's error word and returns, the waits of the boxes
+(fx_jacobi_res.cuh). Here one box stops publishing its faces from one sweep on
+(firex_test_hold_face: a flag that nothing sets) and the wait limit is short
+(firex_set_wait_limit): the neighbours' waits expire, each CTA sets the simulation's error word and returns, the waits of the boxes
 behind them expire in turn, and every CTA of the launch returns. The host must then report
 FIREX_ERR_TIMEOUT at the next sync and poison the handle, as the reference poisons its engine
 after a device loss (FireXEngine.ts:538-542, 2887-2897: later calls throw). The GPU stays
