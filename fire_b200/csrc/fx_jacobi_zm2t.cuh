@@ -39,6 +39,9 @@
 #ifndef FX_T2_ONE_WAITER
 #define FX_T2_ONE_WAITER 1
 #endif
+#ifndef FX_T2_ISSUE_EARLY  // issue a plane's loads right after the step barrier (else at its end)
+#define FX_T2_ISSUE_EARLY 1
+#endif
 
 // Tensor maps of a simulation (FxSimDev::tmap): pressure pair, correction pair, divergence.
 enum { FX_TM_P0 = 0, FX_TM_P1 = 1, FX_TM_C0 = 2, FX_TM_C1 = 3, FX_TM_DIV = 4, FX_TM_COUNT = 5 };
@@ -156,6 +159,11 @@ FXD bool fx_zm2t_tile(const FxSimDev& S, const CUtensorMap* tmP, float* __restri
         __syncthreads();  // planes up to z + 1 landed for every thread; sweep-1 plane z - 1 is
                           // complete, and step z - 1's reads of the slot of plane z - 3 are done
         if (sm.err) break;
+        const int qn = z + FX_T2_AHEAD;  // into the slot of plane z - 3, read last in step z - 1
+        if (FX_T2_ISSUE_EARLY && qn <= qb) {
+            if (t == 0) issue(qn, (qn - qa) % FX_T2_SLOTS);
+            issued = qn;
+        }
         // ---- sweep 2 on plane z - 2 (from the sweep-1 ring)
         {
             const int qz = z - 2;
@@ -211,11 +219,9 @@ FXD bool fx_zm2t_tile(const FxSimDev& S, const CUtensorMap* tmP, float* __restri
                 out[srow * FX_Z2_COLS + hcol] = o;
             }
         }
-        // ---- the loads of plane z + AHEAD, into the slot of plane z - 3 (read last in step z - 1)
-        const int q = z + FX_T2_AHEAD;
-        if (q <= qb) {
-            if (t == 0) issue(q, (q - qa) % FX_T2_SLOTS);
-            issued = q;
+        if (!FX_T2_ISSUE_EARLY && qn <= qb) {  // the loads of plane z + AHEAD at the step's end
+            if (t == 0) issue(qn, (qn - qa) % FX_T2_SLOTS);
+            issued = qn;
         }
         s0 = sp1;
     }

@@ -890,6 +890,9 @@ static void launch_zm2(cudaStream_t s, const FxBatchDev* B, int bricks, int phas
     fxk_jacobi_zm2<PT, ROUND><<<bricks < g ? bricks : g, FX_Z2_THREADS, sizeof(FxZ2Smem<PT>), s>>>(B, phase, launch, zc);
 }
 
+#ifndef FX_T2_L2_PROMOTION
+#define FX_T2_L2_PROMOTION CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+#endif
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time dependency on
 // the driver library).
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -917,8 +920,7 @@ static bool map_field(EncodeTiledFn fn, CUtensorMap* m, void* base, int X, int Y
     const cuuint32_t box[3] = {FX_Z2_COLS, (cuuint32_t)boxY, 1};
     const cuuint32_t elem[3] = {1, 1, 1};
     return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
-              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+              CU_TENSOR_MAP_SWIZZLE_NONE, FX_T2_L2_PROMOTION, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 bool fx_make_tensor_maps(FxSimDev* h) {

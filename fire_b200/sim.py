@@ -303,7 +303,7 @@ class FireXSim(_Handle):
     def set_tiles(self, simulate_by: int, project: int = 0) -> None:
         """Brick shape of the source pass: 32 x simulate_by x (8 / simulate_by) cells (2, 4, 8;
         0: default); `project`: A.PROJECT_FUSED / A.PROJECT_SEPARATE primary projection and
-        residual divergence (A.PROJECT_AUTO: fused)."""
+        residual divergence (A.PROJECT_AUTO: fused below 8 Mi cells)."""
         self._check(self._lib.firex_set_tiles(self._h, int(simulate_by), int(project)))
 
     @property

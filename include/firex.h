@@ -365,7 +365,8 @@ int firex_batch_set_staging(firex_batch* batch, int32_t staging);
  * shaders.ts:151-342) runs one thread per cell of a 32 x simulate_by x (8 / simulate_by) brick,
  * simulate_by = 2, 4 (the default) or 8; 0 restores the default. project: the primary
  * projection and the divergence of its result (the residual's right-hand side,
- * FireXEngine.ts:2256-2257) run as one fused pass (FUSED) or as two (SEPARATE); AUTO = FUSED.
+ * FireXEngine.ts:2256-2257) run as one fused pass (FUSED) or as two (SEPARATE); AUTO fuses
+ * them below 8 Mi cells per batch (the recomputed neighbours then come from L2).
  * Every choice gives identical results; fire_b200/autotune.py times them. A batch's own
  * setting overrides its members' (0 / AUTO: the first member's). */
 #define FIREX_PROJECT_AUTO 0
