@@ -93,6 +93,23 @@ FXD unsigned fx_res_spin_limit(const unsigned* err) {
     return v ? v : FX_RES_SPIN_LIMIT;
 }
 
+// Variant 3 publishes per warp: each warp adds 1 to its box's flag (a release add) once its own
+// face stores are done, so no CTA barrier precedes the publication; a box has published sweep s
+// when its flag reaches FX_RES_WARPS * (s + 1) (the acquire load that sees that count sees
+// every warp's stores: each add heads a release sequence).
+#ifndef FX_RES_WARP_PUBLISH
+#define FX_RES_WARP_PUBLISH 1
+#endif
+#define FX_RES_WARPS (FX_RES_THREADS / 32)
+FXD void fx_red_release_add_u32(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+FXD void fx_res_publish_warp(unsigned* flags, int me, unsigned s, const unsigned* err) {
+    const unsigned* sync = err - 2;
+    if (sync[FX_SYNC_HOLD_BOX] == (unsigned)me + 1 && s >= sync[FX_SYNC_HOLD_SWEEP]) return;
+    fx_red_release_add_u32(flags + me, 1u);
+}
+
 // Publishes box `me`'s faces of sweep s (flag = s + 1, release), unless the host holds them back.
 FXD void fx_res_publish(unsigned* flags, int me, unsigned s, const unsigned* err) {
     const unsigned* sync = fx_res_sync(err);
@@ -500,9 +517,10 @@ FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phas
 // columns, thread t taking interior column (x group, row) t with its z neighbours in
 // registers, its x neighbours from the adjacent lanes (warp shuffles) where those hold
 // the same row and plane.
-// Three CTA barriers per sweep: face stores done (then the flag), old values read and
-// neighbour flags seen (the waiting threads spin before it), new values and halo rows
-// written. Each thread's first halo load is issued before it writes its new values back,
+// Two CTA barriers per sweep: old values read and neighbour flags seen (the waiting threads
+// spin before it), new values and halo rows written; each warp publishes its own face stores
+// with a release add (FX_RES_WARP_PUBLISH; otherwise a third barrier orders the CTA's face
+// stores before one release store). Each thread's first halo load is issued before it writes its new values back,
 // so that L2 round trip overlaps the write-back (0.8 % faster at HD). For boxes whose interior columns fit the threads (planner: at most
 // FX_RES_MAXZ planes per column part).
 template <typename PT, bool ROUND>
@@ -606,8 +624,13 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
             }
         }
         if (!last) {
-            __syncthreads();  // every face store of this CTA precedes the flag (release is cumulative)
-            if (t == 0) fx_res_publish(cx.flags, b, (unsigned)s, cx.err);
+            if (FX_RES_WARP_PUBLISH) {
+                __syncwarp();  // this warp's face stores precede its add (release is cumulative)
+                if ((t & 31) == 0) fx_res_publish_warp(cx.flags, b, (unsigned)s, cx.err);
+            } else {
+                __syncthreads();  // every face store of this CTA precedes the flag
+                if (t == 0) fx_res_publish(cx.flags, b, (unsigned)s, cx.err);
+            }
         }
         float4 nv[FX_RES_MAXZ];
         {
@@ -646,7 +669,8 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         if (!last && t < 4 && cx.nb[t] >= 0) {
             const unsigned limit = fx_res_spin_limit(cx.err);
             unsigned spins = 0;
-            while (fx_ld_acquire_u32(cx.flags + cx.nb[t]) < (unsigned)s + 1) {
+            const unsigned need = FX_RES_WARP_PUBLISH ? FX_RES_WARPS * ((unsigned)s + 1) : (unsigned)s + 1;
+            while (fx_ld_acquire_u32(cx.flags + cx.nb[t]) < need) {
                 if (++spins > limit) {
                     atomicExch(cx.err, 1u);
                     s_flag = 0;
