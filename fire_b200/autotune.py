@@ -33,7 +33,7 @@ class Candidate:
     kernel: str
     block: int = 0
     zchunk: int = 0
-    staging: int = A.STAGING_AUTO  # two-sweep pass: TMA (FP32 pressure) or cp.async
+    staging: int = A.STAGING_AUTO  # two-sweep pass: cp.async (AUTO) or TMA (FP32 pressure)
     simulate_by: int = 0           # source-pass bricks: 32 x by x (8 / by); 0 = default
     project: int = A.PROJECT_AUTO  # primary projection fused with the residual divergence or not
 
@@ -45,7 +45,7 @@ def default_candidates() -> list:
     out = [Candidate("resident", v + 1) for v in (3, 2, 1, 0)]
     out += [Candidate("unblocked")]
     out += [Candidate("zmarch", 0, zc) for zc in (8, 16, 32)]
-    out += [Candidate("fused", 2, zc, st) for zc in (16, 32, 64) for st in (A.STAGING_AUTO, A.STAGING_CPASYNC)]
+    out += [Candidate("fused", 2, zc, st) for zc in (16, 32, 64) for st in (A.STAGING_CPASYNC, A.STAGING_TMA)]
     return out
 
 

@@ -27,7 +27,9 @@
 
 #include "fx_jacobi_zm2.cuh"
 
+#ifndef FX_T2_SLOTS
 #define FX_T2_SLOTS 6
+#endif
 #define FX_T2_AHEAD (FX_T2_SLOTS - 3)  // step z issues the loads of plane z + AHEAD
 #define FX_T2_PBOX_Y FX_Z2_PROWS       // 34 rows of 40 floats
 #define FX_T2_DBOX_Y FX_Z2_RROWS       // 32 rows of 40 floats

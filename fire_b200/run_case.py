@@ -3,7 +3,7 @@
     python -m fire_b200.run_case X Y Z [--steps N] [--jacobi auto|unblocked|zmarch|fused|resident]
                                        [--block K] [--zchunk ZC] [--pressure auto|warm_f32|f16|cold_f32]
                                        [--mixed] [--iters P R] [--profile] [--time N]
-                                       [--staging auto|cpasync] [--project auto|fused|separate]
+                                       [--staging auto|cpasync|tma] [--project auto|fused|separate]
                                        [--simulate-by 2|4|8]
 
 A sphere emitter near the floor (radius X/9), seeded velocity noise and emission jitter,
@@ -35,8 +35,8 @@ def main() -> None:
     ap.add_argument("--iters", type=int, nargs=2, default=(96, 96))
     ap.add_argument("--profile", action="store_true", help="per-pass device times (no graph replay)")
     ap.add_argument("--time", type=int, default=0, help="then time this many steps (graph replay)")
-    ap.add_argument("--staging", default="auto", choices=["auto", "cpasync"],
-                    help="plane staging of the two-sweep pass (auto: TMA with FP32 pressure)")
+    ap.add_argument("--staging", default="auto", choices=["auto", "cpasync", "tma"],
+                    help="plane staging of the two-sweep pass (auto: cp.async)")
     ap.add_argument("--project", default="auto", choices=["auto", "fused", "separate"],
                     help="primary projection and residual divergence in one pass or two")
     ap.add_argument("--simulate-by", type=int, default=0, choices=[0, 2, 4, 8], help="source-pass brick height")
@@ -48,7 +48,7 @@ def main() -> None:
                         spheres=[dict(center=(X / 2, Y / 16, Z / 2), radius=X / 9)])
     s = FireXSim((X, Y, Z), opts)
     s.set_jacobi(a.jacobi, a.block, a.zchunk)
-    s.set_staging(A.STAGING_CPASYNC if a.staging == "cpasync" else A.STAGING_AUTO)
+    s.set_staging({"auto": A.STAGING_AUTO, "cpasync": A.STAGING_CPASYNC, "tma": A.STAGING_TMA}[a.staging])
     s.set_tiles(a.simulate_by, {"auto": A.PROJECT_AUTO, "fused": A.PROJECT_FUSED, "separate": A.PROJECT_SEPARATE}[a.project])
     if a.profile:
         s.set_profiling(True)

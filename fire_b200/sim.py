@@ -296,8 +296,8 @@ class FireXSim(_Handle):
         self._check(self._lib.firex_set_jacobi(self._h, jacobi_kernel(kernel), int(block), int(zchunk)))
 
     def set_staging(self, staging: int) -> None:
-        """How the two-sweep pass stages its planes: A.STAGING_AUTO (TMA when the pressure is
-        FP32) or A.STAGING_CPASYNC."""
+        """How the two-sweep pass stages its planes: A.STAGING_AUTO (cp.async), A.STAGING_CPASYNC
+        or A.STAGING_TMA (tensor tile loads; FP32 pressure only)."""
         self._check(self._lib.firex_set_staging(self._h, int(staging)))
 
     def set_tiles(self, simulate_by: int, project: int = 0) -> None:

@@ -349,15 +349,15 @@ int firex_set_jacobi(firex_sim* sim, int32_t kernel, int32_t block, int32_t zchu
 int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, int32_t zchunk);
 
 /* How the two-sweep pass (FUSED, block 2) brings its pressure and divergence planes into
- * shared memory. AUTO (the default) = TMA when the pressure is FP32: one elected thread per
- * CTA issues tiled tensor loads (cp.async.bulk.tensor) completing on per-slot mbarriers;
- * FP16 pressure (branch B) and CPASYNC use per-thread cp.async copies. Both give the same
- * results bit for bit. A batch's own setting overrides its members' (AUTO: the first
- * member's). No reference counterpart (the reference's tiled solve stages through
- * workgroup memory, shaders.ts:405-459). */
+ * shared memory. TMA (FP32 pressure only): one elected thread per CTA issues tiled tensor
+ * loads (cp.async.bulk.tensor) completing on per-slot mbarriers. CPASYNC: per-thread cp.async
+ * copies. Both give the same results bit for bit. AUTO (the default) = CPASYNC, measured
+ * faster on B200; FP16 pressure (branch B) always uses CPASYNC. A batch's own setting overrides
+ * its members' (AUTO: the first member's). No reference counterpart (the reference's tiled
+ * solve stages through workgroup memory, shaders.ts:405-459). */
 #define FIREX_STAGING_AUTO 0
 #define FIREX_STAGING_CPASYNC 1
-#define FIREX_STAGING_TMA 2   /* reported by firex_get_diagnostics */
+#define FIREX_STAGING_TMA 2
 int firex_set_staging(firex_sim* sim, int32_t staging);
 int firex_batch_set_staging(firex_batch* batch, int32_t staging);
 

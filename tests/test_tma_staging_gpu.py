@@ -1,6 +1,6 @@
 """The two-sweep Jacobi pass with its planes staged by TMA (cp.async.bulk.tensor tile loads on
-mbarriers, fx_jacobi_zm2t.cuh) against the same pass staged by per-thread cp.async copies and
-against single sweeps: bit-identical fields in the FP32 branches (warm-started A, cold-started
+mbarriers, fx_jacobi_zm2t.cuh; selected with STAGING_TMA) against the same pass staged by
+per-thread cp.async copies (AUTO) and against single sweeps: bit-identical fields in the FP32 branches (warm-started A, cold-started
 C, whose first launches of each solve read no input pressure), for grids below, at and above
 one 32 x 30 tile, x extents that end inside a tile, the first and last rows and planes of the
 grid inside the tensor boxes (their out-of-grid rows arrive as zeros and must not be read),
@@ -32,7 +32,7 @@ def pair(dims, opts, zc):
     tma, cp = FireXSim(dims, opts), FireXSim(dims, opts)
     for s in (tma, cp):
         s.set_jacobi("fused", 2, zc)
-    cp.set_staging(A.STAGING_CPASYNC)
+    tma.set_staging(A.STAGING_TMA)
     return tma, cp
 
 
@@ -56,6 +56,7 @@ def test_tma_staging_zero_dt_matches_the_oracle():
     opts = sphere_options(dims, P=16, R=12)
     g, o = FireXSim(dims, opts), OracleSim(dims, opts)
     g.set_jacobi("fused", 2, 8)
+    g.set_staging(A.STAGING_TMA)
     g.step(3, 0.0)
     o.step(3, 0.0)
     assert g.diagnostics["jacobi_staging"] == A.STAGING_TMA
@@ -66,6 +67,7 @@ def test_fp16_pressure_keeps_cp_async_staging():
     dims = (36, 44, 28)
     g = FireXSim(dims, sphere_options(dims, P=8, R=8, pressure_mode=A.PRESSURE_F16))
     g.set_jacobi("fused", 2, 8)
+    g.set_staging(A.STAGING_TMA)
     g.step(1, DT)
     assert g.diagnostics["jacobi_staging"] == A.STAGING_CPASYNC
     g.close()
@@ -80,6 +82,7 @@ def test_tma_batch_of_uneven_grids_equals_each_alone():
         s.step(3, DT)
     with FireXBatch() as b:
         b.set_jacobi("fused", 2, 16)
+        b.set_staging(A.STAGING_TMA)
         for s in members:
             b.add(s)
         b.step(3, DT)
