@@ -81,9 +81,13 @@ def config(extra=None) -> dict:
     return c
 
 
+_NVML_HANDLES: dict = {}
+
+
 class ClockSampler:
     """Samples SM clocks and clock-event (throttle) reasons during a timed region, through
-    NVML every 20 ms (reads only; nvidia-smi every 200 ms where NVML is unavailable)."""
+    NVML every 5 ms (reads only; nvidia-smi every 200 ms where NVML is unavailable). NVML is
+    opened when the sampler is made, so a short timed region starts sampling at once."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -92,7 +96,7 @@ class ClockSampler:
     REASON_BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
                    "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, device_index: int, interval_s: float = 0.02):
+    def __init__(self, device_index: int, interval_s: float = 0.005):
         self.idx = device_index
         self.pci = None  # the CUDA device's PCI address: NVML indices need not follow CUDA's
         try:
@@ -106,6 +110,7 @@ class ClockSampler:
         self._stop = threading.Event()
         self._t = None
         self._nvml = None
+        self._h = self._open()
 
     def _sample_nvml(self, h):
         import pynvml as N
@@ -123,7 +128,11 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         return float(parts[1]), float(parts[2]), {names[i] for i in range(4) if parts[5 + i].lower() == "active"}
 
-    def _run(self):
+    def _open(self):
+        """NVML handle of the CUDA device (opened once per process, before any timed region)."""
+        global _NVML_HANDLES
+        if self.idx in _NVML_HANDLES:
+            return _NVML_HANDLES[self.idx]
         h = None
         try:
             import pynvml as N
@@ -134,9 +143,14 @@ class ClockSampler:
                 h = None
             if h is None:
                 h = N.nvmlDeviceGetHandleByIndex(self.idx)
-            self._nvml = N
         except Exception:
             h = None
+        _NVML_HANDLES[self.idx] = h
+        return h
+
+    def _run(self):
+        h = self._h
+        self._nvml = h
         while True:
             try:
                 s = self._sample_nvml(h) if h is not None else self._sample_smi()
@@ -146,11 +160,6 @@ class ClockSampler:
                 pass
             if self._stop.wait(self.interval if h is not None else 0.2):
                 break
-        if self._nvml is not None:
-            try:
-                self._nvml.nvmlShutdown()
-            except Exception:
-                pass
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -260,6 +269,7 @@ def run_gpu(args) -> None:
     sim = FireXSim(DIMS, options(make_options))
     stream = torch.cuda.ExternalStream(sim.stream)
     n_cells = cells()
+    ClockSampler(dev)  # opens NVML now, outside every timed region
 
     # ---- warm-up ----
     sim.step(args.warmup, DT)
