@@ -42,7 +42,7 @@ class Candidate:
 
 
 def default_candidates() -> list:
-    out = [Candidate("resident", v + 1) for v in (3, 2, 1, 0)]
+    out = [Candidate("resident", v + 1) for v in (4, 3, 2, 1, 0)]
     out += [Candidate("unblocked")]
     out += [Candidate("zmarch", 0, zc) for zc in (8, 16, 32)]
     out += [Candidate("fused", 2, zc, st) for zc in (16, 32, 64) for st in (A.STAGING_CPASYNC, A.STAGING_TMA)]

@@ -240,22 +240,24 @@ bool res_box(int X, int Y, int Z, int m, int variant, FxResBox* out) {
         if (fx_res_smem_bytes(X, by, bz) > FX_RES_SMEM_MAX) continue;
         const long long G = (long long)by * bz * gx;
         double work;
-        if (variant == 3) {
+        if (variant == 3 || variant == 4) {
             // faces dealt out; interior columns (rows off the y faces x groups) one per
-            // thread, split along z when there are fewer columns than threads
-            if (2LL * (by + bz) * gx > (long long)FX_RES_MAXF * FX_RES_THREADS) continue;
+            // thread, split along z when there are fewer columns than threads (variant 4:
+            // the threads but the copy warp)
+            const long long T = variant == 4 ? FX_RES_COPY_TC : FX_RES_THREADS;
+            if (2LL * (by + bz) * gx > (long long)FX_RES_MAXF * T) continue;
             // the most interior rows and planes a box can have: a box with a neighbour on
             // one side only keeps all but one row (plane) off its faces
             const int nbzHere = (Z + bz - 1) / bz;
             const long long rowsI = nby == 1 ? by : by - 1, planesI = nbzHere == 1 ? bz : bz - 1;
             const long long Cmax = rowsI * gx;
-            if (Cmax > FX_RES_THREADS) continue;
-            const long long parts = std::max(1LL, FX_RES_THREADS / std::max(1LL, Cmax));
+            if (Cmax > T) continue;
+            const long long parts = std::max(1LL, T / std::max(1LL, Cmax));
             const long long zlen = (planesI + parts - 1) / parts;
             if (zlen > FX_RES_MAXZ) continue;
             if (zlen < 4) continue;  // short columns: the faces-first variants do better (measured)
             const long long F = 2LL * (by + bz) * gx;
-            work = (double)zlen + (double)((F + FX_RES_THREADS - 1) / FX_RES_THREADS);
+            work = (double)zlen + (double)((F + T - 1) / T);
         } else if (variant != 0) {
             // faces (at most 2 (by + bz) rows of groups) and interior dealt out separately
             const int maxi = variant == 2 ? FX_RES_MAXI_SMALL : FX_RES_MAXI;
@@ -642,11 +644,14 @@ struct firex_batch {
         if (wantRes && !members.empty()) {
             std::vector<std::array<int, 3>> dims;
             for (firex_sim* s : members) dims.push_back({s->X, s->Y, s->Z});
-            // the first variant every member fits: faces first with interior columns (long
-            // columns only), faces first (small-box instance first), then the column variant
-            const int cap = fx_res_capacity(members[0]->half);
-            for (int v : {3, 2, 1, 0}) {
+            // the first variant every member fits: faces first with interior columns and a
+            // copy warp (FP32 pressure; 6.0 against 7.6 us per sweep at HD on B200), the same
+            // without the copy warp (long columns only), faces first (small-box instance
+            // first), then the column variant
+            for (int v : {4, 3, 2, 1, 0}) {
                 if (resForce >= 0 && v != resForce) continue;
+                if (v == 4 && members[0]->half) continue;  // the copy warp moves FP32 rows
+                const int cap = fx_res_capacity(members[0]->half, v);
                 if (res_assign(dims, cap, v, &boxes, &resSmem)) {
                     resOk = true;
                     resVariant = v;
@@ -1656,7 +1661,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
 
 static bool jacobi_args_ok(int32_t kernel, int32_t block, int32_t zchunk) {
     if (kernel < FIREX_JACOBI_AUTO || kernel > FIREX_JACOBI_RESIDENT || zchunk < 0 || zchunk > 4096) return false;
-    if (kernel == FIREX_JACOBI_RESIDENT) return block >= 0 && block <= 4;
+    if (kernel == FIREX_JACOBI_RESIDENT) return block >= 0 && block <= 5;
     return kernel != FIREX_JACOBI_FUSED || block == 2;
 }
 // the block argument kept per kernel: sweeps per launch (FUSED), variant + 1 (RESIDENT)

@@ -35,12 +35,12 @@ void fx_launch_project(cudaStream_t s, bool half, const FxBatchDev* B, int brick
 void fx_launch_project_div(cudaStream_t s, bool half, const FxBatchDev* B, int bricks);
 // Every sweep of a phase in one cooperative launch of `ctas` CTAs with `smem` bytes of
 // dynamic shared memory (fx_jacobi_res.cuh; variant 0 column, 1 faces-first, 2 faces-first
-// for small boxes);
-// fx_res_capacity: the most CTAs one such launch can hold resident on this device (0 when
-// unavailable).
+// for small boxes, 3 faces-first with interior columns, 4 variant 3 with a copy warp);
+// fx_res_capacity: the most CTAs of that variant one such launch can hold resident on this
+// device (0 when unavailable).
 cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, int variant, const FxBatchDev* B, int ctas, int phase,
                                  int smem);
-int fx_res_capacity(bool half);
+int fx_res_capacity(bool half, int variant);
 
 // Single-simulation utilities.
 void fx_launch_init(cudaStream_t s, int storage, const FxSimDev* S, float tAmbient, float oxygen, float noise);

@@ -30,10 +30,12 @@
 // waits for it then expire in turn, every CTA returns, and the host reports a timeout.
 #pragma once
 
+#include "fx_async.cuh"
 #include "fx_step_math.cuh"
 #include "fx_storage.cuh"
 
 #define FX_RES_THREADS 512
+#define FX_RES_COPY_TC (FX_RES_THREADS - 32)  // compute threads of variant 4 (the last warp copies)
 #define FX_RES_MAXG 12                // groups of 4 cells per thread, column variant
 #define FX_RES_MAXF 4                 // face groups per thread, faces-first variant
 #define FX_RES_MAXI 11                // interior groups per thread, faces-first variant
@@ -164,6 +166,16 @@ FXD bool fx_res_exchange(unsigned* flags, int me, const int nb[4], unsigned s, u
     }
     __syncthreads();
     return *flag != 0;
+}
+
+// Bounded wait until a neighbour's flag reaches `need` (acquire). False when it ran out.
+FXD bool fx_r4_wait_flag(const unsigned* flag, unsigned need, unsigned limit) {
+    unsigned spins = 0;
+    while (fx_ld_acquire_u32(flag) < need) {
+        if (++spins > limit) return false;
+        if (spins > 64) __nanosleep(32);
+    }
+    return true;
 }
 
 // Geometry of CTA b's box and its neighbours, and the box's first load.
@@ -512,6 +524,73 @@ FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phas
     }
 }
 
+// Variant 4's copy warp (the CTA's last warp; the other T threads run variant 3's sweep):
+// for every sweep but the last, once the compute warps have read the halo rows of the sweep
+// (they arrive on `faces` after their face groups, the only groups that read them), lanes
+// 0-3 wait for the four neighbours' faces of the sweep (acquire loads of the flags, each
+// bounded), and the lanes issue one bulk copy each of the halo rows and planes from the
+// sweep's output buffer into the halo slots, completing on `halo`; the compute threads wait
+// for that phase before the next sweep. The copies thus run while the interior is computed.
+// Not inlined: its registers then stay out of the compute threads' allocation (inlined, the
+// sweep spills).
+struct FxResCopyBars {
+    unsigned long long faces;  // the compute warps read the sweep's halo (count T / 32)
+    unsigned long long halo;   // the next sweep's halo rows landed (count 1 + transaction bytes)
+};
+static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxResCtx& cx, int phase, int T, FxResCopyBars& bars,
+                       volatile int* abort) {
+    const int n = cx.n, X = cx.X, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, rowsP = cx.rowsP;
+    const long long XY = cx.XY;
+    const int lane = threadIdx.x & 31;
+    const unsigned limit = fx_res_spin_limit(cx.err), nw = (unsigned)T / 32u;
+    const unsigned rowBytes = (unsigned)X * 4u, planeBytes = (unsigned)ny * rowBytes;
+    const int nbMine = lane == 0 ? cx.nb[0] : lane == 1 ? cx.nb[1] : lane == 2 ? cx.nb[2] : lane == 3 ? cx.nb[3] : -1;
+    const unsigned bytes = (unsigned)nz * rowBytes * ((cx.nbLoY ? 1u : 0u) + (cx.nbHiY ? 1u : 0u)) +
+                           planeBytes * ((cx.nbLoZ ? 1u : 0u) + (cx.nbHiZ ? 1u : 0u));
+    int armed = 0;  // sweeps whose halo was requested
+    bool ok = true;
+    for (int s = 0; s + 1 < n; ++s) {
+        const float* pout = reinterpret_cast<const float*>(fx_solve_bufs(S, phase, s).pout);
+        bool mine = fx_mbar_wait_bounded(&bars.faces, (unsigned)s & 1u, limit);
+        if (mine && nbMine >= 0) mine = fx_r4_wait_flag(cx.flags + nbMine, nw * ((unsigned)s + 1u), limit);
+        if (!__all_sync(0xffffffffu, mine)) {
+            ok = false;
+            break;
+        }
+        // the neighbours' face stores, seen through lanes 0-3's acquire loads and the warp
+        // barrier, come before the copies; the compute warps' reads of the slots are ordered
+        // by the faces mbarrier
+        fx_fence_proxy_async_global();
+        if (lane == 0) fx_mbar_expect_tx(&bars.halo, bytes);
+        __syncwarp();
+        armed = s + 1;
+        for (int i = lane; i < 2 * nz + 2; i += 32) {
+            if (i < nz) {
+                if (cx.nbLoY)
+                    fx_bulk_g2s(cx.sp + (i + 1) * rowsP * X, pout + (long long)(z0 + i) * XY + (long long)(y0 - 1) * X,
+                                rowBytes, &bars.halo);
+            } else if (i < 2 * nz) {
+                const int lz = i - nz;
+                if (cx.nbHiY)
+                    fx_bulk_g2s(cx.sp + ((lz + 1) * rowsP + ny + 1) * X,
+                                pout + (long long)(z0 + lz) * XY + (long long)(y0 + ny) * X, rowBytes, &bars.halo);
+            } else if (i == 2 * nz) {
+                if (cx.nbLoZ)
+                    fx_bulk_g2s(cx.sp + X, pout + (long long)(z0 - 1) * XY + (long long)y0 * X, planeBytes, &bars.halo);
+            } else if (cx.nbHiZ) {
+                fx_bulk_g2s(cx.sp + ((nz + 1) * rowsP + 1) * X, pout + (long long)(z0 + nz) * XY + (long long)y0 * X,
+                            planeBytes, &bars.halo);
+            }
+        }
+    }
+    if (!ok && lane == 0) {
+        atomicExch(cx.err, 1u);
+        *abort = 1;
+    }
+    // every copy this warp issued lands before the CTA can end
+    if (armed > 0) fx_mbar_wait_bounded(&bars.halo, (unsigned)(armed - 1) & 1u, limit);
+}
+
 // Faces-first column variant: the face groups are dealt out over all threads as in the
 // faces-first variant and kept in registers (no parking); the interior is walked in z
 // columns, thread t taking interior column (x group, row) t with its z neighbours in
@@ -523,15 +602,21 @@ FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phas
 // stores before one release store). Each thread's first halo load is issued before it writes its new values back,
 // so that L2 round trip overlaps the write-back (0.8 % faster at HD). For boxes whose interior columns fit the threads (planner: at most
 // FX_RES_MAXZ planes per column part).
-template <typename PT, bool ROUND>
+// COPY (variant 4, FP32 pressure): the last warp is a copy warp (fx_res_copier) that waits for
+// the neighbours and brings the halo rows in with bulk copies while the interior is computed;
+// the other FX_RES_COPY_TC threads run the sweep, synchronise on a named barrier, publish per
+// warp, and wait for the copies instead of waiting for flags and loading the halo themselves.
+template <typename PT, bool ROUND, bool COPY>
 FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
     __shared__ int s_flag;
+    __shared__ FxResCopyBars cbars;
+    __shared__ int s_abort;
     const FxResCtx cx = fx_res_setup<PT>(S, bx, b, phase, sm);
     const int n = cx.n, X = cx.X, Y = cx.Y, Z = cx.Z, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, gx = cx.gx;
     const int rowsP = cx.rowsP;
     const long long XY = cx.XY;
     const bool nbLoY = cx.nbLoY, nbHiY = cx.nbHiY, nbLoZ = cx.nbLoZ, nbHiZ = cx.nbHiZ;
-    const int T = blockDim.x, t = threadIdx.x, lane = t & 31;
+    const int T = (int)blockDim.x - (COPY ? 32 : 0), t = threadIdx.x, lane = t & 31;
     float* sp = cx.sp;
     const float* sd = cx.sd;
     const int planeP = rowsP * X, planeD = bx.by * X;
@@ -608,8 +693,28 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         const int fq = g & 0x3ff, fly = (g >> 10) & 0x7ff, flz = g >> 21;
         return ((flz + 1) * rowsP + fly + 1) * X + 4 * fq;
     };
-    if (t == 0) s_flag = 1;
+    // With COPY the face slots pass through an empty asm on every use, so the compiler
+    // recomputes their offsets each sweep instead of keeping them live across the sweep loop
+    // (which spills); without it the plain values compile without spills.
+    auto fresh = [](int g) {
+        if (COPY) asm volatile("" : "+r"(g));
+        return g;
+    };
+    if (t == 0) {
+        s_flag = 1;
+        if (COPY) {
+            fx_mbar_init(&cbars.faces, (unsigned)T / 32u);
+            fx_mbar_init(&cbars.halo, 1);
+            s_abort = 0;
+            asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        }
+    }
     __syncthreads();
+    if (COPY && t >= T) {
+        fx_res_copier(S, cx, phase, T, cbars, &s_abort);
+        return;
+    }
+    const unsigned limit = fx_res_spin_limit(cx.err);
 
     for (int s = 0; s < n; ++s) {
         const bool last = s == n - 1;
@@ -619,12 +724,19 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
 #pragma unroll
         for (int k = 0; k < FX_RES_MAXF; ++k) {
             if (pf[k] >= 0) {
-                nf[k] = update(pf[k]);
-                if (!last) PStore<PT>::st4(pout, gidx(pf[k]), nf[k]);
+                const int g = fresh(pf[k]);
+                nf[k] = update(g);
+                if (!last) PStore<PT>::st4(pout, gidx(g), nf[k]);
             }
         }
         if (!last) {
-            if (FX_RES_WARP_PUBLISH) {
+            if (COPY) {
+                __syncwarp();  // this warp's face stores and halo reads precede its add and arrival
+                if (lane == 0) {
+                    fx_res_publish_warp(cx.flags, b, (unsigned)s, cx.err);
+                    fx_mbar_arrive(&cbars.faces);
+                }
+            } else if (FX_RES_WARP_PUBLISH) {
                 __syncwarp();  // this warp's face stores precede its add (release is cumulative)
                 if ((t & 31) == 0) fx_res_publish_warp(cx.flags, b, (unsigned)s, cx.err);
             } else {
@@ -666,7 +778,7 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         }
         // the neighbours' faces of this sweep: the waiting threads spin before the barrier
         // that also ends every read of the old values
-        if (!last && t < 4 && cx.nb[t] >= 0) {
+        if (!COPY && !last && t < 4 && cx.nb[t] >= 0) {
             const unsigned limit = fx_res_spin_limit(cx.err);
             unsigned spins = 0;
             const unsigned need = FX_RES_WARP_PUBLISH ? FX_RES_WARPS * ((unsigned)s + 1) : (unsigned)s + 1;
@@ -679,10 +791,14 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
                 if (spins > 64) __nanosleep(32);
             }
         }
-        __syncthreads();
-        if (!s_flag) return;  // a wait expired (every thread sees it after the barrier)
+        if (COPY) {
+            if (fx_bar_or(1, T, *reinterpret_cast<volatile int*>(&s_abort) != 0)) return;
+        } else {
+            __syncthreads();
+            if (!s_flag) return;  // a wait expired (every thread sees it after the barrier)
+        }
         // the first halo item's load goes out before the write-back
-        const int hTotal = last ? 0 : fx_res_halo_total(cx);
+        const int hTotal = (last || COPY) ? 0 : fx_res_halo_total(cx);
         float4 h0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         int h0so = -1;
         if (t < hTotal) {
@@ -702,18 +818,25 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
 #pragma unroll
         for (int k = 0; k < FX_RES_MAXF; ++k) {
             if (pf[k] >= 0) {
-                *reinterpret_cast<float4*>(sp + sidx(pf[k])) = nf[k];
-                if (last) PStore<PT>::st4(pout, gidx(pf[k]), nf[k]);
+                const int g = fresh(pf[k]);
+                *reinterpret_cast<float4*>(sp + sidx(g)) = nf[k];
+                if (last) PStore<PT>::st4(pout, gidx(g), nf[k]);
             }
         }
         if (last) break;
-        if (h0so >= 0) *reinterpret_cast<float4*>(sp + h0so) = h0;
-        for (int i = t + T; i < hTotal; i += T) {
-            long long hg;
-            int so;
-            fx_res_halo_item(cx, i, hg, so);
-            *reinterpret_cast<float4*>(sp + so) = fx_res_ld4_cg<PT>(pout, hg);
+        if (COPY) {  // the copy warp's halo rows of this sweep
+            const bool bad = !fx_mbar_wait_bounded(&cbars.halo, (unsigned)s & 1u, limit);
+            if (bad) atomicExch(cx.err, 1u);
+            if (fx_bar_or(1, T, bad || *reinterpret_cast<volatile int*>(&s_abort) != 0)) return;
+        } else {
+            if (h0so >= 0) *reinterpret_cast<float4*>(sp + h0so) = h0;
+            for (int i = t + T; i < hTotal; i += T) {
+                long long hg;
+                int so;
+                fx_res_halo_item(cx, i, hg, so);
+                *reinterpret_cast<float4*>(sp + so) = fx_res_ld4_cg<PT>(pout, hg);
+            }
+            __syncthreads();  // halo rows in place before the next sweep
         }
-        __syncthreads();  // halo rows in place before the next sweep
     }
 }

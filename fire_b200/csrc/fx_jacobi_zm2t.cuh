@@ -25,6 +25,7 @@
 
 #include <cuda.h>
 
+#include "fx_async.cuh"
 #include "fx_jacobi_zm2.cuh"
 
 #ifndef FX_T2_SLOTS
@@ -58,30 +59,6 @@ struct FxT2Smem {
 static_assert(FX_T2_PSLOT * 4 >= FX_T2_PBYTES && (FX_T2_PSLOT * 4) % 128 == 0, "pressure slots: 128-byte aligned");
 static_assert((FX_T2_DSLOT * 4) % 128 == 0, "divergence slots: 128-byte aligned");
 
-FXD unsigned fx_smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-FXD void fx_mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(fx_smem_u32(bar)), "r"(count) : "memory");
-}
-FXD void fx_mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fx_smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-FXD bool fx_mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(fx_smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase with the given parity; false when the limit ran out.
-FXD bool fx_mbar_wait(unsigned long long* bar, unsigned parity, unsigned limit) {
-    for (unsigned i = 0; i < limit; ++i)
-        if (fx_mbar_try_wait(bar, parity)) return true;
-    return false;
-}
 // A 3-D tiled tensor load of the box at (x, y, z) into shared memory, completing on bar.
 FXD void fx_tma_load3(void* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
     asm volatile(

@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(256) fxk_norm_partial(const FxSimDev* __restri
 
 // ---- every sweep of a Jacobi phase in one cooperative launch (fx_jacobi_res.cuh) --------
 // VARIANT: 0 column, 1 faces-first, 2 faces-first for small boxes, 3 faces-first with
-// interior columns (fx_jacobi_res.cuh).
+// interior columns, 4 variant 3 with a copy warp (FP32 pressure) (fx_jacobi_res.cuh).
 template <typename PT, int VARIANT>
 __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatchDev* __restrict__ B, int phase) {
     extern __shared__ float4 fx_res_smem[];
@@ -754,7 +754,10 @@ __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatc
     const int b = w - B->start[FX_SHAPE_RES][si];
     if (VARIANT == 1) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI>(S, B->res[si], b, phase, sm);
     else if (VARIANT == 2) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI_SMALL>(S, B->res[si], b, phase, sm);
-    else if (VARIANT == 3) fx_res_box_v3<PT, sizeof(PT) == 2>(S, B->res[si], b, phase, sm);
+    else if (VARIANT == 3) fx_res_box_v3<PT, sizeof(PT) == 2, false>(S, B->res[si], b, phase, sm);
+    else if (VARIANT == 4) {
+        if constexpr (sizeof(PT) == 4) fx_res_box_v3<float, false, true>(S, B->res[si], b, phase, sm);
+    }
     else fx_res_box_col<PT, sizeof(PT) == 2>(S, B->res[si], b, phase, sm);
 }
 
@@ -965,6 +968,7 @@ static const void* res_fn() {
 }
 static const void* res_kernel(bool half, int variant) {
     switch (variant) {
+        case 4: return half ? nullptr : res_fn<float, 4>();
         case 1: return half ? res_fn<__half, 1>() : res_fn<float, 1>();
         case 2: return half ? res_fn<__half, 2>() : res_fn<float, 2>();
         case 3: return half ? res_fn<__half, 3>() : res_fn<float, 3>();
@@ -972,28 +976,27 @@ static const void* res_kernel(bool half, int variant) {
     }
 }
 
-// Largest resident-Jacobi grid that one cooperative launch can keep resident.
-int fx_res_capacity(bool half) {
-    int cap = 1 << 30;
-    for (int variant = 0; variant < 4; ++variant) {  // every variant: the plan picks one later
-        const void* fn = res_kernel(half, variant);
-        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX) != cudaSuccess) {
-            cudaGetLastError();
-            return 0;
-        }
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FX_RES_THREADS, FX_RES_SMEM_MAX) != cudaSuccess) {
-            cudaGetLastError();
-            return 0;
-        }
-        cap = std::min(cap, per_sm * num_sms());
+// Most CTAs of resident-Jacobi variant `variant` that one cooperative launch can keep
+// resident (0: the variant cannot run, e.g. variant 4 with FP16 pressure).
+int fx_res_capacity(bool half, int variant) {
+    const void* fn = res_kernel(half, variant);
+    if (!fn) return 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
     }
-    return cap;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, FX_RES_THREADS, FX_RES_SMEM_MAX) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm * num_sms();
 }
 
 cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, int variant, const FxBatchDev* B, int ctas, int phase,
                                  int smem) {
     const void* fn = res_kernel(half, variant);
+    if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};

@@ -341,9 +341,11 @@ int firex_set_graphs(firex_sim* sim, int32_t on);
 #define FIREX_JACOBI_FUSED 3
 /* Every sweep of a phase in one cooperative launch with the pressure held in shared
  * memory (only box faces cross L2 between sweeps); used by AUTO whenever the batch fits
- * on chip, else the single-sweep default runs. With RESIDENT, `block` 1-4 restricts the
+ * on chip, else the single-sweep default runs. With RESIDENT, `block` 1-5 restricts the
  * box plan to variant block - 1 (0 columns, 1 faces first, 2 faces first for small
- * boxes, 3 faces first with interior columns); 0 lets the planner choose. */
+ * boxes, 3 faces first with interior columns, 4 variant 3 with a copy warp that brings
+ * the halo rows in by bulk asynchronous copies: FP32 pressure only); 0 lets the planner
+ * choose. */
 #define FIREX_JACOBI_RESIDENT 4
 int firex_set_jacobi(firex_sim* sim, int32_t kernel, int32_t block, int32_t zchunk);
 int firex_batch_set_jacobi(firex_batch* batch, int32_t kernel, int32_t block, int32_t zchunk);

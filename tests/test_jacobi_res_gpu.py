@@ -3,9 +3,9 @@ pressure held in shared memory, box faces exchanged through L2): its fields must
 bit-identical to one sweep per launch in every branch (warm f32, cold f32, f16 storage
 rounded every sweep, mixed storage), for any sweep counts, grids that do and do not
 divide into boxes, and batches whose members share the launch. The grids cover every
-variant the planner picks: faces first (small boxes), and faces first with interior
-columns, one column per thread (128x192x128, 80x120x80) or columns split in z parts
-(96x144x96)."""
+variant the planner picks: faces first (small boxes), faces first with interior columns
+(FP16 pressure, or on request), one column per thread (128x192x128, 80x120x80) or columns
+split in z parts (96x144x96), and the same with a copy warp (FP32 pressure under AUTO)."""
 from __future__ import annotations
 
 import numpy as np
@@ -43,6 +43,20 @@ def pair(dims, opts, steps=3):
 @pytest.mark.parametrize("dims", [(16, 20, 24), (36, 44, 28), (132, 20, 40), (64, 96, 64), (96, 144, 96), (80, 120, 80)])
 def test_resident_equals_single_sweeps(dims, mode):
     one, res = pair(dims, sphere_options(dims, P=12, R=9, pressure_mode=mode))
+    same(one, res)
+
+
+@pytest.mark.parametrize("mode", [A.PRESSURE_WARM_F32, A.PRESSURE_COLD_F32])
+@pytest.mark.parametrize("dims", [(96, 144, 96), (80, 120, 80), (128, 192, 128)])
+def test_variant3_fp32_equals_single_sweeps(dims, mode):
+    """FP32 pressure takes variant 4 under AUTO; variant 3 (block 4) stays selectable."""
+    opts = sphere_options(dims, P=12, R=9, pressure_mode=mode)
+    one, res = FireXSim(dims, opts), FireXSim(dims, opts)
+    one.set_jacobi("unblocked")
+    res.set_jacobi("resident", 4)
+    one.step(2, DT)
+    res.step(2, DT)
+    assert res.diagnostics["jacobi_variant"] == 3
     same(one, res)
 
 

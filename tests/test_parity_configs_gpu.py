@@ -5,8 +5,8 @@ the unblocked Jacobi. These tests compare the CUDA path with the oracle directly
 picks the other kernels:
 
   * the HD tier (128x192x128, sphere r=14 at (64,12,64), +-10 % jitter, 96+96 sweeps), the
-    benchmark's workload, where AUTO runs the resident Jacobi (box variant 3: faces first,
-    interior columns);
+    benchmark's workload, where AUTO runs the resident Jacobi (box variant 4: faces first,
+    interior columns, halo rows brought in by a copy warp);
   * 508x508x36 (9,290,304 cells, above the 8 Mi-cell threshold), where AUTO runs two sweeps
     per HBM pass (the z-marching two-sweep kernel with 16-plane chunks; 36 planes leave a
     partial chunk), in branch A (FP32) and branch B (FP16 pressure, pressureShaders.ts:62-117).
@@ -60,7 +60,7 @@ def test_hd_step_against_the_oracle(hd_state, dt):
     g.step(1, dt)
     o.step(1, dt)
     d = g.diagnostics
-    assert d["jacobi_kernel"] == A.JACOBI_RESIDENT and d["jacobi_variant"] == 3, d
+    assert d["jacobi_kernel"] == A.JACOBI_RESIDENT and d["jacobi_variant"] == 4, d
     assert g.state == o.state
     if dt == 0.0:
         fields_equal(g, o)
