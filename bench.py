@@ -111,13 +111,21 @@ class ClockSampler:
         self._t = None
         self._nvml = None
         self._h = self._open()
+        # the maximum SM clock is a constant and its query takes milliseconds (the current
+        # clock and the reasons about 0.3 ms together): read it once, outside the timed region
+        self._max_mhz = None
+        if self._h is not None:
+            try:
+                import pynvml as N
+                self._max_mhz = float(N.nvmlDeviceGetMaxClockInfo(self._h, N.NVML_CLOCK_SM))
+            except Exception:
+                self._h = None
 
     def _sample_nvml(self, h):
         import pynvml as N
         sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
-        mx = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
         bits = N.nvmlDeviceGetCurrentClocksEventReasons(h)
-        return float(sm), float(mx), {k for k, b in self.REASON_BITS.items() if bits & b}
+        return float(sm), self._max_mhz, {k for k, b in self.REASON_BITS.items() if bits & b}
 
     def _sample_smi(self):
         out = subprocess.run(["nvidia-smi", "-i", self.pci or str(self.idx), f"--query-gpu={self.QUERY}",

@@ -169,7 +169,7 @@ FXD bool fx_res_exchange(unsigned* flags, int me, const int nb[4], unsigned s, u
 }
 
 // Bounded wait until a neighbour's flag reaches `need` (acquire). False when it ran out.
-FXD bool fx_r4_wait_flag(const unsigned* flag, unsigned need, unsigned limit) {
+FXD bool fx_res_wait_flag(const unsigned* flag, unsigned need, unsigned limit) {
     unsigned spins = 0;
     while (fx_ld_acquire_u32(flag) < need) {
         if (++spins > limit) return false;
@@ -552,7 +552,7 @@ static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxRes
     for (int s = 0; s + 1 < n; ++s) {
         const float* pout = reinterpret_cast<const float*>(fx_solve_bufs(S, phase, s).pout);
         bool mine = fx_mbar_wait_bounded(&bars.faces, (unsigned)s & 1u, limit);
-        if (mine && nbMine >= 0) mine = fx_r4_wait_flag(cx.flags + nbMine, nw * ((unsigned)s + 1u), limit);
+        if (mine && nbMine >= 0) mine = fx_res_wait_flag(cx.flags + nbMine, nw * ((unsigned)s + 1u), limit);
         if (!__all_sync(0xffffffffu, mine)) {
             ok = false;
             break;
