@@ -182,6 +182,7 @@ def declare_firex(lib: C.CDLL) -> None:
         "firex_destroy": (C.c_int, [vp]),
         "firex_last_error": (C.c_char_p, [vp]),
         "firex_set_parameter": (C.c_int, [vp, C.c_char_p, C.c_int32, C.c_double]),
+        "firex_set_params": (C.c_int, [vp, C.POINTER(C.c_float)]),
         "firex_get_parameter": (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_double)]),
         "firex_reset": (C.c_int, [vp]),
         "firex_step": (C.c_int, [vp, C.c_int32, C.c_double]),
@@ -236,7 +237,7 @@ def declare_firex(lib: C.CDLL) -> None:
 # Entry points the header declares; the CPU suite checks the built library exports them.
 HEADER_SYMBOLS = [
     "firex_default_options", "firex_field_element_size", "firex_create", "firex_destroy",
-    "firex_last_error", "firex_set_parameter", "firex_get_parameter", "firex_reset", "firex_step",
+    "firex_last_error", "firex_set_parameter", "firex_set_params", "firex_get_parameter", "firex_reset", "firex_step",
     "firex_sync", "firex_read_field", "firex_read_field_async", "firex_write_field", "firex_divergence_norm",
     "firex_set_render_packing", "firex_render_volumes", "firex_read_particles", "firex_write_particles",
     "firex_divergence_norm_noalloc", "firex_set_wait_limit", "firex_test_hold_face", "firex_get_state",

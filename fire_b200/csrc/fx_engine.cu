@@ -1331,6 +1331,33 @@ int firex_set_parameter(firex_sim* s, const char* name, int32_t kind, double val
     return FIREX_OK;
 }
 
+int firex_set_params(firex_sim* s, const float* p) {
+    if (!s || !p) return FIREX_ERR_BAD_ARG;
+    if (p[0] != (float)s->X || p[1] != (float)s->Y || p[2] != (float)s->Z)
+        return s->fail(FIREX_ERR_BAD_ARG, "parameter block: grid slots differ from the handle's dimensions");
+    // the parameter slots of the block (the layout build_params writes)
+    static const struct {
+        int slot;
+        const char* name;
+    } kSlots[] = {{8, "fuelRate"},        {9, "oxygenRate"},      {10, "heatEfficiency"},    {11, "vorticity"},
+                  {12, "waterFlow"},      {13, "sprayAngle"},     {14, "waterEnabled"},      {16, "cameraYaw"},
+                  {17, "cameraPitch"},    {18, "cameraDistance"}, {24, "viewMode"},          {25, "aimHeight"},
+                  {26, "nozzleType"},     {27, "exposure"},       {28, "burnerSize"},        {29, "burnerDepth"},
+                  {30, "sourceThickness"}, {31, "firePower"},     {32, "domainWidth"},       {33, "domainHeight"},
+                  {34, "domainDepth"},    {36, "sourceLift"},     {37, "buoyancyScale"},     {38, "flamePersistence"},
+                  {39, "viewZoom"},       {40, "airEntrainment"}, {41, "frontDefinition"},   {43, "opticalDetailTarget"}};
+    for (const auto& e : kSlots) {
+        const int i = param_slot(e.name);
+        double v = p[e.slot];
+        int kind = FIREX_VALUE_NUMBER;
+        if (e.slot == 13) v = v * 180.0 / M_PI;  // the block holds radians, the parameter degrees
+        if (e.slot == 14) kind = FIREX_VALUE_BOOLEAN;
+        s->named[i] = apply_rule(kParams[i], s->named[i], kind, v);
+    }
+    s->refresh_params();
+    return FIREX_OK;
+}
+
 int firex_get_parameter(const firex_sim* s, const char* name, double* value) {
     if (!s || !name || !value) return FIREX_ERR_BAD_ARG;
     int i = param_slot(name);

@@ -247,6 +247,12 @@ class FireXSim(_Handle):
     def __init__(self, dims: Iterable[int], options: A.Options | None = None, **kw):
         super().__init__(load_library(), dims, options, **kw)
 
+    def set_params(self, block) -> None:
+        """Every parameter from a 44-float uniform block (the layout of `uniforms()` and of
+        the reference's writeUniforms); the grid slots must match this simulation."""
+        arr = np.ascontiguousarray(np.asarray(block, dtype=np.float32).reshape(A.UNIFORM_FLOATS))
+        self._check(self._lib.firex_set_params(self._h, arr.ctypes.data_as(C.POINTER(C.c_float))))
+
     def set_render_packing(self, on: bool) -> None:
         """Pack the three FP16 render volumes at the end of every step (qualityShaders.ts)."""
         self._check(self._lib.firex_set_render_packing(self._h, 1 if on else 0))

@@ -153,6 +153,16 @@ const char* firex_last_error(const firex_sim* sim);
 int firex_set_parameter(firex_sim* sim, const char* name, int32_t kind, double value);
 int firex_get_parameter(const firex_sim* sim, const char* name, double* value);
 
+/* Every parameter at once from a 44-float block in the layout of the reference's uniform
+ * buffer (Parameters, shaders.ts:2-14, as FireXEngine.writeUniforms fills it,
+ * FireXEngine.ts:2043-2113; firex_get_uniforms returns the same layout). Each parameter slot
+ * goes through the rules of firex_set_parameter (clamps, rounding, thresholds, booleans; the
+ * spray angle is read in radians). The grid slots 0-2 must equal the handle's dimensions,
+ * else FIREX_ERR_BAD_ARG and nothing changes. The time slots (dt, simulation time, frame),
+ * the fixed ambient temperature, the canvas and particle slots and the cinematic flag are the
+ * handle's own (firex_step, firex_set_state, the creation options) and are not read. */
+int firex_set_params(firex_sim* sim, const float params[FIREX_UNIFORM_FLOATS]);
+
 /* Re-initialises every field and the counters (FireXEngine.reset, FireXEngine.ts:843-852,
  * initializeFields :1933-1974). */
 int firex_reset(firex_sim* sim);
