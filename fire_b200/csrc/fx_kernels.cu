@@ -98,7 +98,26 @@ struct Acc {
 template <class St, int BY>
 __global__ void __launch_bounds__(256, 3) fxk_simulate(const FxBatchDev* __restrict__ B) {
     constexpr int BX = FX_CELL_BX, BZ = 256 / (FX_CELL_BX * BY);
+    // the simulation's parameter block, the uniform entries of its per-step table and its
+    // constant divisors, read by every cell: staged in shared memory when the CTA's brick
+    // changes simulation (shared loads instead of about 80 global loads per cell)
+    __shared__ FxParams sP;
+    __shared__ float sUT[TU_COUNT];
+    __shared__ FxDivc sDC[DIVC_COUNT];
+    const FxSimDev* cur = nullptr;
     fx_for_bricks<FX_SHAPE_CELL>(B, [&](const FxSimDev& S, int b) {
+        if (&S != cur) {      // the same brick, so the same decision, in every thread
+            __syncthreads();  // every read of the previous simulation's block is done
+            constexpr int nP = sizeof(FxParams) / 4, nD = sizeof(sDC) / 4;
+            static_assert(sizeof(FxParams) % 4 == 0 && nP + TU_COUNT + nD <= 1024, "staging words");
+            for (int i = threadIdx.x; i < nP + TU_COUNT + nD; i += blockDim.x) {
+                if (i < nP) reinterpret_cast<uint32_t*>(&sP)[i] = reinterpret_cast<const uint32_t*>(&S.prm)[i];
+                else if (i < nP + TU_COUNT) sUT[i - nP] = S.tab[i - nP];
+                else reinterpret_cast<uint32_t*>(sDC)[i - nP - TU_COUNT] = reinterpret_cast<const uint32_t*>(S.divc)[i - nP - TU_COUNT];
+            }
+            __syncthreads();
+            cur = &S;
+        }
         const int nbx = (S.X + BX - 1) / BX, nby = (S.Y + BY - 1) / BY;
         const int x = (b % nbx) * BX + threadIdx.x % BX;
         const int y = ((b / nbx) % nby) * BY + (threadIdx.x / BX) % BY;
@@ -106,7 +125,7 @@ __global__ void __launch_bounds__(256, 3) fxk_simulate(const FxBatchDev* __restr
         if (x >= S.X || y >= S.Y || z >= S.Z) return;
         const FxGrid g{S.X, S.Y, S.Z};
         Acc<St> a{S.flow[S.fi], S.species[S.si], S.liquid};
-        FxCellOut o = fx_simulate_cell(S.prm, g, x, y, z, a, S.tab, S.divc);
+        FxCellOut o = fx_simulate_cell(sP, g, x, y, z, a, S.tab, sUT, sDC);
         const int id = x + S.X * (y + S.Y * z);
         fx_st_flow(S.flow[S.fi ^ 1], id, o.flow);
         St::st_species(S.species[S.si ^ 1], id, o.species);

@@ -42,7 +42,7 @@ FXD float fx_div_by_const(float x, float d, float rcp) { return fx_div_range(x, 
 // engine did not enable carries lo = +inf, so every x takes the IEEE division of
 // fx_div_range's rare path (zeros keep their sign): one 16-byte load, no flag.
 FXD float fx_divc(float x, const FxDivc& c) {
-    const float4 v = __ldg(reinterpret_cast<const float4*>(&c));  // d, rcp, lo, hi
+    const float4 v = *reinterpret_cast<const float4*>(&c);  // d, rcp, lo, hi
     return fx_div_range(x, v.x, v.y, v.z, v.w);
 }
 
@@ -249,9 +249,12 @@ struct FxCellOut {
 // simulate (shaders.ts:151-342) for cell (x, y, z): advection, diffusion, source,
 // boundary ambient, liquid cooling, entrainment, Arrhenius burn, vorticity confinement,
 // turbulence, buoyancy, spray momentum, radiation, open-top outflow and wall clamps.
+// P, ut (the per-step table's uniform entries, TU_*) and dc are the same for every cell of a
+// simulation: the source pass stages them in shared memory; tab (the per-coordinate tables)
+// and the fields come from global memory.
 template <class Acc>
 FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y, int z, const Acc& a,
-                               const float* __restrict__ tab, const FxDivc* __restrict__ dc) {
+                               const float* __restrict__ tab, const float* ut, const FxDivc* dc) {
     const float* u = P.u;
     const int X = g.X, Y = g.Y, Z = g.Z;
     const FxTabLayout L = fx_tab_layout(X, Y, Z);
@@ -260,7 +263,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     float dt = u[U_DT];
 
     float4 orig = a.flow(id);
-    const float3 metric = make_float3(__ldg(tab + TU_MX), __ldg(tab + TU_MY), __ldg(tab + TU_MZ));
+    const float3 metric = make_float3(ut[TU_MX], ut[TU_MY], ut[TU_MZ]);
     float btx = picx - orig.x * dt * metric.x;
     float bty = picy - orig.y * dt * metric.y;
     float btz = picz - orig.z * dt * metric.z;
@@ -282,12 +285,12 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         float vax = fx_divc(left.x + right.x + bottom.x + top.x + back.x + front.x, dc[DIVC_SIX]);
         float vay = fx_divc(left.y + right.y + bottom.y + top.y + back.y + front.y, dc[DIVC_SIX]);
         float vaz = fx_divc(left.z + right.z + bottom.z + top.z + back.z + front.z, dc[DIVC_SIX]);
-        float vm = __ldg(tab + TU_VMIX);
+        float vm = ut[TU_VMIX];
         flow.x = fx_mix(flow.x, vax, vm);
         flow.y = fx_mix(flow.y, vay, vm);
         flow.z = fx_mix(flow.z, vaz, vm);
         float ta = fx_divc(left.w + right.w + bottom.w + top.w + back.w + front.w, dc[DIVC_SIX]);
-        flow.w = fx_mix(flow.w, ta, __ldg(tab + TU_TMIX));
+        flow.w = fx_mix(flow.w, ta, ut[TU_TMIX]);
     }
     {  // species diffusion (shaders.ts:182-187)
         float4 sl = a.species(oL), sr = a.species(oR);
@@ -297,13 +300,13 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
                                  fx_divc(sl.y + sr.y + sb.y + st.y + sk.y + sf.y, dc[DIVC_SIX]),
                                  fx_divc(sl.z + sr.z + sb.z + st.z + sk.z + sf.z, dc[DIVC_SIX]),
                                  fx_divc(sl.w + sr.w + sb.w + st.w + sk.w + sf.w, dc[DIVC_SIX]));
-        species = fx_mix4(species, avg, __ldg(tab + TU_SMIX));
+        species = fx_mix4(species, avg, ut[TU_SMIX]);
     }
 
     // Source injection (shaders.ts:189-201); the sphere list replaces the burner.
-    const float firePower = __ldg(tab + TU_POWER);
-    const float powerRoot = __ldg(tab + TU_POWER_ROOT);
-    const float thermalPower = __ldg(tab + TU_THERMAL);
+    const float firePower = ut[TU_POWER];
+    const float powerRoot = ut[TU_POWER_ROOT];
+    const float thermalPower = ut[TU_THERMAL];
     float source;
     if (P.emitter_mode == FIREX_EMITTER_SPHERES) {
         source = 0.0f;
@@ -321,7 +324,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         const float cellular = FC(0.76) + FC(0.24) * __ldg(tab + L.x + TX_CELL * X + x) * __ldg(tab + L.z + TZ_CELL * Z + z);
         const float lobeArg = __ldg(tab + L.x + TX_LOBE * X + x) * __ldg(tab + L.z + TZ_LOBE * Z + z);
         const float lobes = fx_mix(FC(0.48), FC(1.18), fx_smoothstep_c(FC(-0.42), lobeArg, dc[DIVC_LOBE]));
-        const float texture = fx_mix(cellular, cellular * lobes, __ldg(tab + TU_CINE));
+        const float texture = fx_mix(cellular, cellular * lobes, ut[TU_CINE]);
         const float pulse = __ldg(tab + L.pulse + z * X + x);
         source = expf(-(radial + vertical)) * texture * pulse;
         species.x = fx_max(species.x, source * u[U_FUEL_RATE] * firePower);
@@ -335,7 +338,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         flow.x = flow.x + swx * s;
         flow.y = flow.y + swy * s;
         flow.z = flow.z + swz * s;
-        flow.y += source * dt * FC(0.52) * __ldg(tab + TU_LIFT) * powerRoot;
+        flow.y += source * dt * FC(0.52) * ut[TU_LIFT] * powerRoot;
     }
 
     if (x == 0 || x == X - 1 || z == 0 || z == Z - 1 || y == Y - 1) {  // shaders.ts:203-208
@@ -357,8 +360,8 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     }
 
     // O2 entrainment (shaders.ts:220-232)
-    const float entrainment = __ldg(tab + TU_ENTRAIN);
-    const float ambientOxygen = __ldg(tab + TU_AMB_O2);
+    const float entrainment = ut[TU_ENTRAIN];
+    const float ambientOxygen = ut[TU_AMB_O2];
     float oxygenDeficit = fx_clamp(fx_divc(ambientOxygen - species.y, dc[DIVC_AMBIENT_O2]), 0.0f, 1.0f);
     float fuelCore = fx_smoothstep_c(FC(0.30), species.x, dc[DIVC_FUELCORE]);
     float interfaceWeight = oxygenDeficit * fx_mix(1.0f, FC(0.18), fuelCore);
@@ -394,7 +397,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     species.y = fx_max(0.0f, oxygenBefore - burn * 4.0f);
     species.z = fx_clamp(species.z + burn * (1.0f + richness * FC(1.8)), 0.0f, 3.0f);
     species.w = fx_clamp(species.w + burn * FC(0.62), 0.0f, 3.0f);
-    flow.w += burn * __ldg(tab + TU_HEAT);
+    flow.w += burn * ut[TU_HEAT];
     float reaction = fx_clamp(fx_divc(burn, dc[DIVC_DT]) * FC(0.22), 0.0f, 4.0f);
 
     {  // vorticity confinement: curl x grad(T) (shaders.ts:258-272)
@@ -408,7 +411,7 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         gx = gx / gl;
         gy = gy / gl;
         gz = gz / gl;
-        const float vs = __ldg(tab + TU_VORT_S);
+        const float vs = ut[TU_VORT_S];
         flow.x = flow.x + (gy * cz - gz * cy) * vs;
         flow.y = flow.y + (gz * cx - gx * cz) * vs;
         flow.z = flow.z + (gx * cy - gy * cx) * vs;
@@ -419,18 +422,18 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
         float ltx = __ldg(tab + L.ltx + z * Y + y);
         float lty = __ldg(tab + L.lty + z * X + x);
         float ltz = __ldg(tab + L.ltz + y * X + x);
-        float ts = __ldg(tab + TU_TURB) * hotPlume * heightEnvelope * dt;
+        float ts = ut[TU_TURB] * hotPlume * heightEnvelope * dt;
         flow.x = flow.x + ltx * ts;
         flow.y = flow.y + lty * ts;
         flow.z = flow.z + ltz * ts;
     }
     {  // buoyancy (shaders.ts:287-288)
         float buoyancy = fx_clamp(fx_divc(flow.w - u[U_T_AMBIENT], dc[DIVC_BUOYANCY]), FC(-0.1), FC(1.2));
-        flow.y += buoyancy * dt * FC(0.72) * __ldg(tab + TU_BUOY);
+        flow.y += buoyancy * dt * FC(0.72) * ut[TU_BUOY];
     }
     if (liquidRaw) species.z *= expf(-water * dt * FC(4.8));  // exp(-0) == 1 exactly otherwise
     {  // spray momentum (shaders.ts:293-297)
-        const float dx = __ldg(tab + TU_SPRAY_X), dy = __ldg(tab + TU_SPRAY_Y), dz = __ldg(tab + TU_SPRAY_Z);
+        const float dx = ut[TU_SPRAY_X], dy = ut[TU_SPRAY_Y], dz = ut[TU_SPRAY_Z];
         flow.x = flow.x + dx * water * dt * FC(0.82);
         flow.y = flow.y + dy * water * dt * FC(0.82);
         flow.z = flow.z + dz * water * dt * FC(0.82);
@@ -439,12 +442,12 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     // pow(T, 4): cells at exactly the ambient temperature (every cold cell clamped to it
     // above) take the per-step table value, which is the same powf of the same input
     const float tRad = fx_max(flow.w, 0.0f);
-    const float tamb4 = __ldg(tab + TU_TAMB4);
+    const float tamb4 = ut[TU_TAMB4];
     const float t4 = tRad == u[U_T_AMBIENT] ? tamb4 : powf(tRad, 4.0f);
     float radiation = fx_divc(FC(5.67e-8) * (tamb4 - t4), dc[DIVC_RADIATION]);
     flow.w = fx_max(u[U_T_AMBIENT], flow.w + dt * radiation);
-    species.z *= __ldg(tab + TU_DECAY_Z);
-    species.w *= __ldg(tab + TU_DECAY_W);
+    species.z *= ut[TU_DECAY_Z];
+    species.w *= ut[TU_DECAY_W];
 
     // open-top outflow (shaders.ts:308-321)
     float outflow = __ldg(tab + L.y + TY_OUT * Y + y);
