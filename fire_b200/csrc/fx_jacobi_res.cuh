@@ -190,7 +190,7 @@ struct FxResCtx {
 };
 
 template <typename PT>
-FXD FxResCtx fx_res_setup(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
+FXD FxResCtx fx_res_setup(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm, bool load = true) {
     FxResCtx c;
     c.n = phase == 0 ? S.P : S.R;
     c.X = S.X;
@@ -216,6 +216,7 @@ FXD FxResCtx fx_res_setup(const FxSimDev& S, const FxResBox& bx, int b, int phas
     c.nb[3] = c.nbHiZ ? b + bx.nby : -1;
     c.flags = S.sync + FX_RES_FLAGS + phase * FX_RES_MAX_CTAS;
     c.err = S.sync + 2;
+    if (!load) return c;  // variant 4's copy warp loads the box (fx_res_boot)
     // the box with its halo rows (clamped rows outside the grid are never read) and its divergence
     const FxSolveBufs b0 = fx_solve_bufs(S, phase, 0);
     const int gx = c.gx, ny = c.ny, nz = c.nz, X = c.X;
@@ -536,7 +537,54 @@ FXD void fx_res_box_early(const FxSimDev& S, const FxResBox& bx, int b, int phas
 struct FxResCopyBars {
     unsigned long long faces;  // the compute warps read the sweep's halo (count T / 32)
     unsigned long long halo;   // the next sweep's halo rows landed (count 1 + transaction bytes)
+    unsigned long long boot;   // the box's first load landed (count 1 + transaction bytes)
 };
+
+// Variant 4's compute threads before the first sweep: clear the box when the phase starts from
+// zero, then wait for the copy warp's first load (false when the wait ran out; the error word is
+// then set). Not inlined, as fx_res_boot.
+static __device__ __noinline__ bool fx_res_boot_wait(const FxSimDev& S, const FxResCtx& cx, int phase, int T,
+                                                     unsigned long long* bar) {
+    if (fx_solve_bufs(S, phase, 0).zeroIn) {
+        const int n4 = (cx.nz + 2) * cx.rowsP * cx.gx;
+        for (int i = threadIdx.x; i < n4; i += T) reinterpret_cast<float4*>(cx.sp)[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    const bool ok = fx_mbar_wait_bounded(bar, 0u, fx_res_spin_limit(cx.err));
+    if (!ok) atomicExch(cx.err, 1u);
+    return ok;
+}
+
+// Variant 4's first load of the box, by the copy warp: per plane of the box and its halo that
+// lies in the grid, one bulk copy of its rows y0 - 1 .. y0 + ny that lie in the grid (they are
+// contiguous in the field and in the box), and per plane one copy of the divergence rows,
+// completing on `boot`. Rows and planes outside the grid are never read by the sweep (the walls
+// take the cell itself, the top row is 0), so they are not loaded. A phase that starts from
+// zero loads no pressure (the compute threads clear the box). The warp waits for its copies.
+static __device__ __noinline__ void fx_res_boot(const FxSimDev& S, const FxResBox& bx, const FxResCtx& cx, int phase,
+                                                unsigned long long* bar) {
+    const int lane = threadIdx.x & 31;
+    const FxSolveBufs b0 = fx_solve_bufs(S, phase, 0);
+    const float* pin = reinterpret_cast<const float*>(b0.pin);
+    const int X = cx.X, Y = cx.Y, Z = cx.Z, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, rowsP = cx.rowsP;
+    const long long XY = cx.XY;
+    const int ylo = max(y0 - 1, 0), yhi = min(y0 + ny + 1, Y);
+    const int zlo = max(z0 - 1, 0), zhi = min(z0 + nz + 1, Z);
+    const unsigned pBytes = (unsigned)(yhi - ylo) * (unsigned)X * 4u, dBytes = (unsigned)ny * (unsigned)X * 4u;
+    const int np = b0.zeroIn ? 0 : zhi - zlo;
+    if (lane == 0) fx_mbar_expect_tx(bar, (unsigned)np * pBytes + (unsigned)nz * dBytes);
+    __syncwarp();
+    for (int i = lane; i < np + nz; i += 32) {
+        if (i < np) {
+            const int z = zlo + i, lz = z - z0;
+            fx_bulk_g2s(cx.sp + ((lz + 1) * rowsP + (ylo - y0 + 1)) * X, pin + (long long)z * XY + (long long)ylo * X, pBytes,
+                        bar);
+        } else {
+            const int lz = i - np;
+            fx_bulk_g2s(cx.sd + lz * bx.by * X, S.div + (long long)(z0 + lz) * XY + (long long)y0 * X, dBytes, bar);
+        }
+    }
+    fx_mbar_wait_bounded(bar, 0u, fx_res_spin_limit(cx.err));
+}
 static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxResCtx& cx, int phase, int T, FxResCopyBars& bars,
                        volatile int* abort) {
     const int n = cx.n, X = cx.X, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, rowsP = cx.rowsP;
@@ -611,7 +659,7 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
     __shared__ int s_flag;
     __shared__ FxResCopyBars cbars;
     __shared__ int s_abort;
-    const FxResCtx cx = fx_res_setup<PT>(S, bx, b, phase, sm);
+    const FxResCtx cx = fx_res_setup<PT>(S, bx, b, phase, sm, !COPY);
     const int n = cx.n, X = cx.X, Y = cx.Y, Z = cx.Z, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, gx = cx.gx;
     const int rowsP = cx.rowsP;
     const long long XY = cx.XY;
@@ -705,16 +753,19 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         if (COPY) {
             fx_mbar_init(&cbars.faces, (unsigned)T / 32u);
             fx_mbar_init(&cbars.halo, 1);
+            fx_mbar_init(&cbars.boot, 1);
             s_abort = 0;
             asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         }
     }
     __syncthreads();
     if (COPY && t >= T) {
+        fx_res_boot(S, bx, cx, phase, &cbars.boot);
         fx_res_copier(S, cx, phase, T, cbars, &s_abort);
         return;
     }
     const unsigned limit = fx_res_spin_limit(cx.err);
+    if (COPY && fx_bar_or(1, T, !fx_res_boot_wait(S, cx, phase, T, &cbars.boot))) return;
 
     for (int s = 0; s < n; ++s) {
         const bool last = s == n - 1;
