@@ -548,6 +548,13 @@ static __device__ __noinline__ bool fx_res_boot_wait(const FxSimDev& S, const Fx
     if (fx_solve_bufs(S, phase, 0).zeroIn) {
         const int n4 = (cx.nz + 2) * cx.rowsP * cx.gx;
         for (int i = threadIdx.x; i < n4; i += T) reinterpret_cast<float4*>(cx.sp)[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    } else if (cx.y0 + cx.ny == cx.Y) {
+        // the row above the grid: the top row's update is 0 whatever it reads there, but its
+        // numerators should not meet stale bits (NaN would send them to the slow division)
+        for (int i = threadIdx.x; i < (cx.nz + 2) * cx.gx; i += T) {
+            const int lz = i / cx.gx, q = i - lz * cx.gx;
+            reinterpret_cast<float4*>(cx.sp + (lz * cx.rowsP + cx.ny + 1) * cx.X)[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
     }
     const bool ok = fx_mbar_wait_bounded(bar, 0u, fx_res_spin_limit(cx.err));
     if (!ok) atomicExch(cx.err, 1u);
