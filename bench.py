@@ -51,10 +51,30 @@ E2E_MIN_STEPS = 200
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each Jacobi
 # kernel on this workload, from one ncu capture of that kernel (the same command as this
 # benchmark's default run, one launch captured).
-JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25244416 + 621824}
+JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25259264 + 459008}
+# The two-sweep pass at 508^3 (too large for a capture): one pass (2 sweeps) of a 508x508x128
+# capture moved 266.7 MB + 104.2 MB of DRAM for 33,032,192 cells; the 508^3 figure scales it by
+# the cell count (its traffic grows in proportion: the same tiles and chunks over more planes).
+ZM2_CAPTURE_BYTES, ZM2_CAPTURE_CELLS = 266.7e6 + 104.2e6, 508 * 508 * 128
 
 JACOBI_KERNEL_NAMES = {1: "fxk_jacobi<float>", 2: "fxk_jacobi_zm<float>", 3: "fxk_jacobi_zm2<float>",
                        4: "fxk_jacobi_res<float>"}
+
+
+def zm2_roofline(jac: dict, cells: int, peak: float, peak_kind: str) -> dict:
+    """The two-sweep pass at 508^3 against the copy bandwidth: algorithmic bytes per launch
+    (2 sweeps x 12 B x cells) over the average launch time from the per-pass events, and the
+    DRAM traffic of a launch scaled from the 508x508x128 capture."""
+    launches = jac.get("launches_per_step") or 0
+    if not launches or not jac.get("ms_per_step"):
+        return {}
+    us = jac["ms_per_step"] / launches * 1e3
+    alg = 2 * JACOBI_BYTES_PER_CELL * cells
+    achieved = alg / (us / 1e6) / 1e9
+    return {"roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "avg_launch_us": us, "algorithmic_bytes_per_launch": alg,
+                         "traffic": ZM2_CAPTURE_BYTES * cells / ZM2_CAPTURE_CELLS,
+                         "traffic_note": "dram bytes of one launch at 508x508x128 (ncu), scaled by the cell count"}}
 
 
 def jacobi_kernel_name(diag: dict) -> str:
@@ -598,7 +618,7 @@ def measure_508(warmup: int = 3, steps: int = STEPS_508) -> dict:
                      "target_frac": 0.70},
         "passes": per_pass, "profiled_steps": prof,
         "jacobi": {"kernel": jacobi_kernel_name(diag), "block": diag.get("jacobi_block"),
-                   "zchunk": diag.get("jacobi_zchunk")},
+                   "zchunk": diag.get("jacobi_zchunk"), **zm2_roofline(per_pass["jacobi"], n, peak, peak_kind)},
         "launches_per_step": diag.get("launches_per_step"),
         "clocks": clk.summary(),
     }
