@@ -735,7 +735,7 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
         const float4 pkv = *reinterpret_cast<const float4*>((fz > 0 ? rowC - planeP : rowC) + fx0);
         const float4 pfv = *reinterpret_cast<const float4*>((fz < Z - 1 ? rowC + planeP : rowC) + fx0);
         const float4 d = *reinterpret_cast<const float4*>(sd + (flz * bx.by + fly) * X + fx0);
-        float4 o = fx_jacobi4<true>(c2, pl, pc, pr, pb, pt, pkv, pfv, d);
+        float4 o = fx_jacobi4<true, COPY>(c2, pl, pc, pr, pb, pt, pkv, pfv, d);
         if (ROUND) o = make_float4(PStore<__half>::round(o.x), PStore<__half>::round(o.y), PStore<__half>::round(o.z),
                                    PStore<__half>::round(o.w));
         return o;
@@ -825,7 +825,7 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
                     const float pl = shflL ? fromL : (hasL ? sp[off - 1] : pc.x);
                     const float pr = shflR ? fromR : (hasR ? sp[off + 4] : pc.w);
                     const float4 d = *reinterpret_cast<const float4*>(sd + offD + k * planeD);
-                    float4 o = fx_jacobi4<true>(c2, pl, pc, pr, pb, pt, pk, pfv, d);
+                    float4 o = fx_jacobi4<true, COPY>(c2, pl, pc, pr, pb, pt, pk, pfv, d);
                     if (ROUND) o = make_float4(PStore<__half>::round(o.x), PStore<__half>::round(o.y),
                                                PStore<__half>::round(o.z), PStore<__half>::round(o.w));
                     nv[k] = top ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : o;

@@ -10,6 +10,40 @@
 
 #include "fx_device.cuh"
 
+// ---- packed FP32 pairs (add/sub/mul/fma .rn.f32x2, Blackwell): each lane is rounded
+// exactly as the scalar IEEE operation, so pairing changes no result bit.
+typedef unsigned long long fx_f2;
+FXD fx_f2 fx_pack2(float a, float b) {
+    fx_f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+FXD float2 fx_unpack2(fx_f2 v) {
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return make_float2(a, b);
+}
+FXD fx_f2 fx_add2(fx_f2 a, fx_f2 b) {
+    fx_f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+FXD fx_f2 fx_sub2(fx_f2 a, fx_f2 b) {
+    fx_f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+FXD fx_f2 fx_mul2(fx_f2 a, fx_f2 b) {
+    fx_f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+FXD fx_f2 fx_fma2(fx_f2 a, fx_f2 b, fx_f2 c) {
+    fx_f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
 // Division by a constant d > 0 given rcp = RN(1/d): Markstein's correction step
 // (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
 // processor", IBM J. Res. Dev. 34(1), 1990): q = RN(x*rcp), e = x - q*d exactly by one
@@ -503,40 +537,6 @@ FXD float fx_jacobi_numerator(const FxJacobiConst& c, float l, float r, float b,
                                __fmul_rn(c.wz, __fadd_rn(k, f))),
                      div);
 }
-// ---- packed FP32 pairs (add/sub/mul/fma .rn.f32x2, Blackwell): each lane is rounded
-// exactly as the scalar IEEE operation, so pairing changes no result bit.
-typedef unsigned long long fx_f2;
-FXD fx_f2 fx_pack2(float a, float b) {
-    fx_f2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-FXD float2 fx_unpack2(fx_f2 v) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    return make_float2(a, b);
-}
-FXD fx_f2 fx_add2(fx_f2 a, fx_f2 b) {
-    fx_f2 r;
-    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-FXD fx_f2 fx_sub2(fx_f2 a, fx_f2 b) {
-    fx_f2 r;
-    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-FXD fx_f2 fx_mul2(fx_f2 a, fx_f2 b) {
-    fx_f2 r;
-    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
-    return r;
-}
-FXD fx_f2 fx_fma2(fx_f2 a, fx_f2 b, fx_f2 c) {
-    fx_f2 r;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
-    return r;
-}
-
 // Jacobi constants as pairs, for fx_jacobi4.
 struct FxJacobiConst2 {
     fx_f2 rcp, negDenom;
@@ -547,35 +547,10 @@ FXD FxJacobiConst2 fx_jacobi_const2(const FxJacobiConst& c, float rcp, bool fast
     return FxJacobiConst2{fx_pack2(rcp, rcp), fx_pack2(-c.denom, -c.denom), c.wx, c.wy, c.wz, c.denom, rcp, fast};
 }
 
-// Four consecutive x cells of one Jacobi sweep (the operations of fx_jacobi_numerator and
-// fx_div_by_const, cell by cell, two cells per instruction): pc holds the cells, l and r
-// their outer x neighbours, pb/pt/pk/pf the y-1, y+1, z-1, z+1 rows, d the divergence.
-// A group with a numerator outside the checked range takes the IEEE division for its four
-// cells (the same quotients: inside the range the checked path equals it), through the
-// out-of-line rare path of fx_div_by_const, or inline (INLINE_RARE: no call in the caller's
-// loop; measured faster in the resident kernel at HD, 5.60 against 6.02 us per sweep, and
-// 1 % slower in the two-sweep kernel at 508^3).
-template <bool INLINE_RARE = false>
-FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, float4 pb, float4 pt, float4 pk, float4 pf,
-                      float4 d) {
-    const fx_f2 mid = fx_pack2(pc.y, pc.z);
-    const fx_f2 lr01 = fx_add2(fx_pack2(l, pc.x), mid);
-    const fx_f2 lr23 = fx_add2(mid, fx_pack2(pc.w, r));
-    const fx_f2 bt01 = fx_add2(fx_pack2(pb.x, pb.y), fx_pack2(pt.x, pt.y));
-    const fx_f2 bt23 = fx_add2(fx_pack2(pb.z, pb.w), fx_pack2(pt.z, pt.w));
-    const fx_f2 kf01 = fx_add2(fx_pack2(pk.x, pk.y), fx_pack2(pf.x, pf.y));
-    const fx_f2 kf23 = fx_add2(fx_pack2(pk.z, pk.w), fx_pack2(pf.z, pf.w));
-    // The weight products stay scalar: a packed multiply feeding a packed add is contracted
-    // into a packed fma by the code generator (measured on B200), which rounds once instead
-    // of twice. Scalar mul.rn is never contracted.
-    const float2 s01 = fx_unpack2(lr01), s23 = fx_unpack2(lr23), u01 = fx_unpack2(bt01), u23 = fx_unpack2(bt23);
-    const float2 v01 = fx_unpack2(kf01), v23 = fx_unpack2(kf23);
-    const fx_f2 x01 = fx_pack2(__fmul_rn(c.wxS, s01.x), __fmul_rn(c.wxS, s01.y));
-    const fx_f2 x23 = fx_pack2(__fmul_rn(c.wxS, s23.x), __fmul_rn(c.wxS, s23.y));
-    const fx_f2 y01 = fx_pack2(__fmul_rn(c.wyS, u01.x), __fmul_rn(c.wyS, u01.y));
-    const fx_f2 y23 = fx_pack2(__fmul_rn(c.wyS, u23.x), __fmul_rn(c.wyS, u23.y));
-    const fx_f2 z01 = fx_pack2(__fmul_rn(c.wzS, v01.x), __fmul_rn(c.wzS, v01.y));
-    const fx_f2 z23 = fx_pack2(__fmul_rn(c.wzS, v23.x), __fmul_rn(c.wzS, v23.y));
+// The end of fx_jacobi4 from the six weighted pair sums: the numerators and the division.
+template <bool INLINE_RARE>
+FXD float4 fx_jacobi4_finish(const FxJacobiConst2& c, fx_f2 x01, fx_f2 x23, fx_f2 y01, fx_f2 y23, fx_f2 z01, fx_f2 z23,
+                             float4 d) {
     const fx_f2 n01 = fx_sub2(fx_add2(fx_add2(x01, y01), z01), fx_pack2(d.x, d.y));
     const fx_f2 n23 = fx_sub2(fx_add2(fx_add2(x23, y23), z23), fx_pack2(d.z, d.w));
     const float2 a = fx_unpack2(n01), b = fx_unpack2(n23);
@@ -596,6 +571,51 @@ FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, floa
     }
     return make_float4(fx_div_by_const(a.x, c.denom, c.rcpS), fx_div_by_const(a.y, c.denom, c.rcpS),
                        fx_div_by_const(b.x, c.denom, c.rcpS), fx_div_by_const(b.y, c.denom, c.rcpS));
+}
+
+// Four consecutive x cells of one Jacobi sweep (the operations of fx_jacobi_numerator and
+// fx_div_by_const, cell by cell, two cells per instruction): pc holds the cells, l and r
+// their outer x neighbours, pb/pt/pk/pf the y-1, y+1, z-1, z+1 rows, d the divergence.
+// A group with a numerator outside the checked range takes the IEEE division for its four
+// cells (the same quotients: inside the range the checked path equals it), through the
+// out-of-line rare path of fx_div_by_const, or inline (INLINE_RARE: no call in the caller's
+// loop; measured faster in the resident kernel at HD, 5.60 against 6.02 us per sweep, and
+// 1 % slower in the two-sweep kernel at 508^3).
+// A packed multiply feeding a packed add is contracted into a packed fma by the code
+// generator (measured on B200), which rounds once instead of twice, so the weight products
+// are either scalar multiplies (never contracted) or, with PACKED_W, packed fused
+// multiply-adds of -0: RN(w s + -0) = RN(w s) for every w and s, zeros' signs included, and
+// an fma feeding an add is not contracted. The -0 is computed from the run-time divisor
+// (finite), so the fma cannot be folded back into a multiply. PACKED_W measured 5.61
+// against 5.65 us per sweep in the resident kernel with the copy warp at HD, and 1 % slower
+// per step in the two-sweep kernel at 508^3.
+template <bool INLINE_RARE = false, bool PACKED_W = false>
+FXD float4 fx_jacobi4(const FxJacobiConst2& c, float l, float4 pc, float r, float4 pb, float4 pt, float4 pk, float4 pf,
+                      float4 d) {
+    const fx_f2 mid = fx_pack2(pc.y, pc.z);
+    const fx_f2 lr01 = fx_add2(fx_pack2(l, pc.x), mid);
+    const fx_f2 lr23 = fx_add2(mid, fx_pack2(pc.w, r));
+    const fx_f2 bt01 = fx_add2(fx_pack2(pb.x, pb.y), fx_pack2(pt.x, pt.y));
+    const fx_f2 bt23 = fx_add2(fx_pack2(pb.z, pb.w), fx_pack2(pt.z, pt.w));
+    const fx_f2 kf01 = fx_add2(fx_pack2(pk.x, pk.y), fx_pack2(pf.x, pf.y));
+    const fx_f2 kf23 = fx_add2(fx_pack2(pk.z, pk.w), fx_pack2(pf.z, pf.w));
+    if constexpr (PACKED_W) {
+        const float nzs = -0.0f * fabsf(c.denom);
+        const fx_f2 nz = fx_pack2(nzs, nzs);
+        const fx_f2 wx2 = fx_pack2(c.wxS, c.wxS), wy2 = fx_pack2(c.wyS, c.wyS), wz2 = fx_pack2(c.wzS, c.wzS);
+        return fx_jacobi4_finish<INLINE_RARE>(c, fx_fma2(wx2, lr01, nz), fx_fma2(wx2, lr23, nz), fx_fma2(wy2, bt01, nz),
+                                              fx_fma2(wy2, bt23, nz), fx_fma2(wz2, kf01, nz), fx_fma2(wz2, kf23, nz), d);
+    } else {
+        const float2 s01 = fx_unpack2(lr01), s23 = fx_unpack2(lr23), u01 = fx_unpack2(bt01), u23 = fx_unpack2(bt23);
+        const float2 v01 = fx_unpack2(kf01), v23 = fx_unpack2(kf23);
+        const fx_f2 x01 = fx_pack2(__fmul_rn(c.wxS, s01.x), __fmul_rn(c.wxS, s01.y));
+        const fx_f2 x23 = fx_pack2(__fmul_rn(c.wxS, s23.x), __fmul_rn(c.wxS, s23.y));
+        const fx_f2 y01 = fx_pack2(__fmul_rn(c.wyS, u01.x), __fmul_rn(c.wyS, u01.y));
+        const fx_f2 y23 = fx_pack2(__fmul_rn(c.wyS, u23.x), __fmul_rn(c.wyS, u23.y));
+        const fx_f2 z01 = fx_pack2(__fmul_rn(c.wzS, v01.x), __fmul_rn(c.wzS, v01.y));
+        const fx_f2 z23 = fx_pack2(__fmul_rn(c.wzS, v23.x), __fmul_rn(c.wzS, v23.y));
+        return fx_jacobi4_finish<INLINE_RARE>(c, x01, x23, y01, y23, z01, z23, d);
+    }
 }
 
 // One cell of fx_jacobi4 (the same numerator; the checked constant division when enabled).
