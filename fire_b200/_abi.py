@@ -156,7 +156,8 @@ class Diagnostics(C.Structure):
         ("jacobi_staging", C.c_int32),
         ("simulate_by", C.c_int32),
         ("project_fused", C.c_int32),
-        ("reserved", C.c_int32 * 6),
+        ("project_resident", C.c_int32),
+        ("reserved", C.c_int32 * 5),
     ]
 
 

@@ -141,15 +141,20 @@ struct StepPlan {
     bool res = false;         // every sweep of a phase in one resident launch
     int resVariant = 0;       // ... by this variant of the kernel
     int resSmem = 0;          // its dynamic shared memory per CTA
+    bool projRes = false;     // the residual projection inside the resident launch (variant 4)
     int bricks[FX_NSHAPES] = {};
     auto key() const {
         return std::tie(storage, half, pmode, maxP, maxR, k, zc, zmZc, row4, fuseP, fuseR, pack, tma, simBy, projDiv, res,
-                        resVariant, resSmem,
+                        resVariant, resSmem, projRes,
                         bricks[0],
                         bricks[1], bricks[2], bricks[3], bricks[4], bricks[5], bricks[6]);
     }
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
 };
+
+#ifndef FX_PROJ_RES
+#define FX_PROJ_RES 1  // the residual projection as the resident variant 4's epilogue when it can
+#endif
 
 // A phase of n sweeps may fuse k sweeps per launch when every member runs the same n
 // and the launch count (n/k fused + n%k single) has the parity of n: the result then
@@ -166,7 +171,9 @@ int jacobi_phase_launches(const StepPlan& pl, int phase) {
 void enqueue_jacobi_phase(cudaStream_t st, const StepPlan& pl, FxBatchDev* B, int phase) {
     const int n = phase == 0 ? pl.maxP : pl.maxR;
     if (pl.res) {  // a failed launch is reported by the caller's cudaGetLastError
-        if (n > 0) fx_launch_jacobi_res(st, pl.half, pl.resVariant, B, pl.bricks[FX_SHAPE_RES], phase, pl.resSmem);
+        if (n > 0)
+            fx_launch_jacobi_res(st, pl.half, pl.resVariant, B, pl.bricks[FX_SHAPE_RES], phase, pl.resSmem,
+                                 phase == 1 && pl.projRes);
         return;
     }
     const bool fuse = phase == 0 ? pl.fuseP : pl.fuseR;
@@ -198,7 +205,7 @@ void enqueue_step_launches(cudaStream_t st, const StepPlan& pl, FxBatchDev* B) {
         fx_launch_divergence(st, B, pl.bricks[FX_SHAPE_ROW4], 1);
     }
     enqueue_jacobi_phase(st, pl, B, 1);
-    fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 1);
+    if (!pl.projRes) fx_launch_project(st, pl.half, B, pl.bricks[FX_SHAPE_ROW4], 1);
     fx_launch_step_end(st, B);
     if (pl.pack) fx_launch_pack_batch(st, B, pl.bricks[FX_SHAPE_ROW4]);
 }
@@ -767,6 +774,15 @@ struct firex_batch {
             p.k = 1;
             p.fuseP = p.fuseR = false;
             p.tma = false;
+            // the residual projection as variant 4's epilogue (unless the projection passes are
+            // asked to run separately): every member runs residual sweeps, and every top box has
+            // two rows or more (its top row projects the row below from the box)
+            bool epi = FX_PROJ_RES && resVariant == 4 && pf != FIREX_PROJECT_SEPARATE;
+            for (size_t i = 0; i < members.size() && epi; ++i) {
+                const FxResBox& bx = h->res[i];
+                epi = members[i]->h.R >= 1 && members[i]->Y - (bx.nby - 1) * bx.by >= 2;
+            }
+            p.projRes = epi;
         }
         if (p.k != 2) p.tma = false;
         for (int j = 0; j < FX_NSHAPES; ++j) p.bricks[j] = h->total[j];
@@ -839,8 +855,10 @@ struct firex_batch {
         }
         enqueue_jacobi_phase(stream, pl, d, 1);
         mark(FIREX_PASS_JACOBI, jacobi_phase_launches(pl, 1));
-        fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 1);
-        mark(FIREX_PASS_PROJECT, 1);
+        if (!pl.projRes) {
+            fx_launch_project(stream, pl.half, d, pl.bricks[FX_SHAPE_ROW4], 1);
+            mark(FIREX_PASS_PROJECT, 1);
+        }
         fx_launch_step_end(stream, d);
         if (pl.pack) fx_launch_pack_batch(stream, d, pl.bricks[FX_SHAPE_ROW4]);
         mark(FIREX_PASS_OTHER, pl.pack ? 2 : 1);
@@ -909,7 +927,7 @@ struct firex_batch {
                 pendingLaunches[FIREX_PASS_SIMULATE] += 1;
                 pendingLaunches[FIREX_PASS_DIVERGENCE] += pl.projDiv ? 1 : 2;
                 pendingLaunches[FIREX_PASS_JACOBI] += jacobi_phase_launches(pl, 0) + jacobi_phase_launches(pl, 1);
-                pendingLaunches[FIREX_PASS_PROJECT] += 2;
+                pendingLaunches[FIREX_PASS_PROJECT] += pl.projRes ? 1 : 2;
                 pendingLaunches[FIREX_PASS_PARTICLES] += sph_launches(pl);
             }
         }
@@ -1675,7 +1693,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_zchunk = p.k > 1 ? p.zc : (p.row4 ? 0 : p.zmZc);
     out->graph = b->lastGraph ? 1 : 0;
     out->launches_per_step =
-        (p.projDiv ? 7 : 8) + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) +
+        (p.projDiv ? 7 : 8) - (p.projRes ? 1 : 0) + (p.pack ? 1 : 0) + sph_launches(p) + jacobi_phase_launches(p, 0) +
         jacobi_phase_launches(p, 1);
     out->jacobi_kernel = p.res ? FIREX_JACOBI_RESIDENT
                                : (p.k > 1 ? FIREX_JACOBI_FUSED : (p.row4 ? FIREX_JACOBI_UNBLOCKED : FIREX_JACOBI_ZMARCH));
@@ -1683,6 +1701,7 @@ int firex_get_diagnostics(const firex_sim* s, firex_diagnostics* out) {
     out->jacobi_staging = p.tma ? FIREX_STAGING_TMA : (p.k == 2 ? FIREX_STAGING_CPASYNC : -1);
     out->simulate_by = p.simBy;
     out->project_fused = p.projDiv ? 1 : 0;
+    out->project_resident = p.projRes ? 1 : 0;
     return FIREX_OK;
 }
 

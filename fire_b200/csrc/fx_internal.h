@@ -37,9 +37,10 @@ void fx_launch_project_div(cudaStream_t s, bool half, const FxBatchDev* B, int b
 // dynamic shared memory (fx_jacobi_res.cuh; variant 0 column, 1 faces-first, 2 faces-first
 // for small boxes, 3 faces-first with interior columns, 4 variant 3 with a copy warp);
 // fx_res_capacity: the most CTAs of that variant one such launch can hold resident on this
-// device (0 when unavailable).
+// device (0 when unavailable). epi (variant 4, residual phase): the launch also projects the
+// flow with the final correction (fx_res_project_epi), replacing fx_launch_project's phase 1.
 cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, int variant, const FxBatchDev* B, int ctas, int phase,
-                                 int smem);
+                                 int smem, bool epi);
 int fx_res_capacity(bool half, int variant);
 
 // Single-simulation utilities.

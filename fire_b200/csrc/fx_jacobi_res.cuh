@@ -593,7 +593,7 @@ static __device__ __noinline__ void fx_res_boot(const FxSimDev& S, const FxResBo
     fx_mbar_wait_bounded(bar, 0u, fx_res_spin_limit(cx.err));
 }
 static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxResCtx& cx, int phase, int T, FxResCopyBars& bars,
-                       volatile int* abort) {
+                       volatile int* abort, bool epi) {
     const int n = cx.n, X = cx.X, y0 = cx.y0, z0 = cx.z0, ny = cx.ny, nz = cx.nz, rowsP = cx.rowsP;
     const long long XY = cx.XY;
     const int lane = threadIdx.x & 31;
@@ -604,7 +604,8 @@ static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxRes
                            planeBytes * ((cx.nbLoZ ? 1u : 0u) + (cx.nbHiZ ? 1u : 0u));
     int armed = 0;  // sweeps whose halo was requested
     bool ok = true;
-    for (int s = 0; s + 1 < n; ++s) {
+    // with the projection epilogue, the last sweep's faces are fetched too (its halo rows)
+    for (int s = 0; s + (epi ? 0 : 1) < n; ++s) {
         const float* pout = reinterpret_cast<const float*>(fx_solve_bufs(S, phase, s).pout);
         bool mine = fx_mbar_wait_bounded(&bars.faces, (unsigned)s & 1u, limit);
         if (mine && nbMine >= 0) mine = fx_res_wait_flag(cx.flags + nbMine, nw * ((unsigned)s + 1u), limit);
@@ -646,6 +647,57 @@ static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxRes
     if (armed > 0) fx_mbar_wait_bounded(&bars.halo, (unsigned)(armed - 1) & 1u, limit);
 }
 
+// Variant 4's projection epilogue of the residual phase (projectVelocity with the correction,
+// fxk_project phase 1, with its operations): after the last sweep the box holds the final
+// correction and its halo rows the neighbours' final faces, so each group of 4 cells of a box
+// row reads its flow from global memory and writes the projected flow, every pressure from
+// shared memory. The top row takes the projection of the row below (the planner gives the top
+// box at least two rows, so that row and its plane in front are in the box or its halo).
+// Not inlined: it keeps the sweep's register allocation.
+static __device__ __noinline__ void fx_res_project_epi(const FxSimDev& S, const FxResCtx& cx, int T) {
+    const float4* __restrict__ flowIn = reinterpret_cast<const float4*>(S.flow[S.fi]);
+    float4* __restrict__ flowOut = reinterpret_cast<float4*>(S.flow[S.fi ^ 1]);
+    const float3 m = fx_metric(S.prm.u);
+    const int X = cx.X, Y = cx.Y, Z = cx.Z, gx = cx.gx, ny = cx.ny, rowsP = cx.rowsP;
+    const long long XY = cx.XY;
+    const int planeP = rowsP * X;
+    const int total = ny * cx.nz * gx;
+    for (int i = threadIdx.x; i < total; i += T) {
+        const int q = i % gx, r = i / gx, ly = r % ny, lz = r / ny;
+        const int y = cx.y0 + ly, z = cx.z0 + lz, x0 = 4 * q;
+        const bool topRow = y == Y - 1;
+        const long long c = (long long)z * XY + (long long)y * X + x0;
+        const long long cs = topRow ? c - X : c;  // top row: the projected row below
+        const float* rowS = cx.sp + ((lz + 1) * rowsP + (topRow ? ly - 1 : ly) + 1) * X;
+        const float4 pc4 = *reinterpret_cast<const float4*>(rowS + x0);
+        const float p4 = x0 + 4 < X ? rowS[x0 + 4] : 0.0f;
+        const float4 pt4 = *reinterpret_cast<const float4*>(rowS + X + x0);
+        const float4 pf4 = z < Z - 1 ? *reinterpret_cast<const float4*>(rowS + planeP + x0) : pc4;
+        float4 f[4], sv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) f[j] = __ldg(flowIn + c + j);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) sv[j] = topRow ? __ldg(flowIn + cs + j) : f[j];
+        const float pcs[5] = {pc4.x, pc4.y, pc4.z, pc4.w, p4};
+        const float pts[4] = {pt4.x, pt4.y, pt4.z, pt4.w}, pfs[4] = {pf4.x, pf4.y, pf4.z, pf4.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int x = x0 + j;
+            const float pc = pcs[j];
+            const float px = x + 1 < X ? pcs[j + 1] : pc;
+            const float gxv = (px - pc) * m.x;
+            const float gyv = (pts[j] - pc) * m.y;
+            const float gzv = (pfs[j] - pc) * m.z;
+            float4 o = make_float4(sv[j].x - gxv, sv[j].y - gyv, sv[j].z - gzv, f[j].w);
+            if (x == 0 || x == X - 1) o.x = 0.0f;
+            if (z == 0 || z == Z - 1) o.z = 0.0f;
+            if (y == 0) o.y = 0.0f;
+            if (y == Y - 1) o.y = fx_max(0.0f, o.y);
+            flowOut[c + j] = o;
+        }
+    }
+}
+
 // Faces-first column variant: the face groups are dealt out over all threads as in the
 // faces-first variant and kept in registers (no parking); the interior is walked in z
 // columns, thread t taking interior column (x group, row) t with its z neighbours in
@@ -661,8 +713,9 @@ static __device__ __noinline__ void fx_res_copier(const FxSimDev& S, const FxRes
 // the neighbours and brings the halo rows in with bulk copies while the interior is computed;
 // the other FX_RES_COPY_TC threads run the sweep, synchronise on a named barrier, publish per
 // warp, and wait for the copies instead of waiting for flags and loading the halo themselves.
-template <typename PT, bool ROUND, bool COPY>
+template <typename PT, bool ROUND, bool COPY, bool EPI = false>
 FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, float* sm) {
+    constexpr bool epi = EPI;
     __shared__ int s_flag;
     __shared__ FxResCopyBars cbars;
     __shared__ int s_abort;
@@ -768,7 +821,7 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
     __syncthreads();
     if (COPY && t >= T) {
         fx_res_boot(S, bx, cx, phase, &cbars.boot);
-        fx_res_copier(S, cx, phase, T, cbars, &s_abort);
+        fx_res_copier(S, cx, phase, T, cbars, &s_abort, epi);
         return;
     }
     const unsigned limit = fx_res_spin_limit(cx.err);
@@ -784,10 +837,10 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
             if (pf[k] >= 0) {
                 const int g = fresh(pf[k]);
                 nf[k] = update(g);
-                if (!last) PStore<PT>::st4(pout, gidx(g), nf[k]);
+                if (!last || epi) PStore<PT>::st4(pout, gidx(g), nf[k]);
             }
         }
-        if (!last) {
+        if (!last || epi) {
             if (COPY) {
                 __syncwarp();  // this warp's face stores and halo reads precede its add and arrival
                 if (lane == 0) {
@@ -878,14 +931,18 @@ FXD void fx_res_box_v3(const FxSimDev& S, const FxResBox& bx, int b, int phase, 
             if (pf[k] >= 0) {
                 const int g = fresh(pf[k]);
                 *reinterpret_cast<float4*>(sp + sidx(g)) = nf[k];
-                if (last) PStore<PT>::st4(pout, gidx(g), nf[k]);
+                if (last && !epi) PStore<PT>::st4(pout, gidx(g), nf[k]);
             }
         }
-        if (last) break;
+        if (last && !epi) break;
         if (COPY) {  // the copy warp's halo rows of this sweep
             const bool bad = !fx_mbar_wait_bounded(&cbars.halo, (unsigned)s & 1u, limit);
             if (bad) atomicExch(cx.err, 1u);
             if (fx_bar_or(1, T, bad || *reinterpret_cast<volatile int*>(&s_abort) != 0)) return;
+            if (last) {  // epi: the final box and halo in place
+                fx_res_project_epi(S, cx, T);
+                break;
+            }
         } else {
             if (h0so >= 0) *reinterpret_cast<float4*>(sp + h0so) = h0;
             for (int i = t + T; i < hTotal; i += T) {

@@ -761,7 +761,8 @@ __global__ void __launch_bounds__(256) fxk_norm_partial(const FxSimDev* __restri
 // ---- every sweep of a Jacobi phase in one cooperative launch (fx_jacobi_res.cuh) --------
 // VARIANT: 0 column, 1 faces-first, 2 faces-first for small boxes, 3 faces-first with
 // interior columns, 4 variant 3 with a copy warp (FP32 pressure) (fx_jacobi_res.cuh).
-template <typename PT, int VARIANT>
+// EPI (variant 4, residual phase): the projection epilogue (fx_res_project_epi).
+template <typename PT, int VARIANT, bool EPI = false>
 __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatchDev* __restrict__ B, int phase) {
     extern __shared__ float4 fx_res_smem[];
     const int w = blockIdx.x;
@@ -775,7 +776,7 @@ __global__ void __launch_bounds__(FX_RES_THREADS, 1) fxk_jacobi_res(const FxBatc
     else if (VARIANT == 2) fx_res_box_early<PT, sizeof(PT) == 2, FX_RES_MAXI_SMALL>(S, B->res[si], b, phase, sm);
     else if (VARIANT == 3) fx_res_box_v3<PT, sizeof(PT) == 2, false>(S, B->res[si], b, phase, sm);
     else if (VARIANT == 4) {
-        if constexpr (sizeof(PT) == 4) fx_res_box_v3<float, false, true>(S, B->res[si], b, phase, sm);
+        if constexpr (sizeof(PT) == 4) fx_res_box_v3<float, false, true, EPI>(S, B->res[si], b, phase, sm);
     }
     else fx_res_box_col<PT, sizeof(PT) == 2>(S, B->res[si], b, phase, sm);
 }
@@ -1013,8 +1014,8 @@ int fx_res_capacity(bool half, int variant) {
 }
 
 cudaError_t fx_launch_jacobi_res(cudaStream_t s, bool half, int variant, const FxBatchDev* B, int ctas, int phase,
-                                 int smem) {
-    const void* fn = res_kernel(half, variant);
+                                 int smem, bool epi) {
+    const void* fn = (epi && variant == 4 && !half) ? (const void*)fxk_jacobi_res<float, 4, true> : res_kernel(half, variant);
     if (!fn) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, FX_RES_SMEM_MAX);
     if (e != cudaSuccess) return e;

@@ -399,7 +399,8 @@ typedef struct firex_diagnostics {
     int32_t jacobi_staging;   /* two-sweep pass: FIREX_STAGING_TMA or _CPASYNC it ran; else -1 */
     int32_t simulate_by;      /* source-pass bricks of 32 x simulate_by x (8 / simulate_by) cells */
     int32_t project_fused;    /* 1: the primary projection and the residual divergence ran as one pass */
-    int32_t reserved[6];
+    int32_t project_resident; /* 1: the residual projection ran inside the resident Jacobi's launch */
+    int32_t reserved[5];
 } firex_diagnostics;
 int firex_get_diagnostics(const firex_sim* sim, firex_diagnostics* out);
 

@@ -123,3 +123,60 @@ def test_variant4_withheld_face_expires_the_waits():
     o.step(2, 0.0)
     same(h, o)
     h.close()
+
+
+# ---- the residual projection as the resident launch's epilogue (fx_res_project_epi) ----------
+
+@pytest.mark.parametrize("dims,P,R", [((128, 192, 128), 96, 96), ((96, 144, 96), 12, 1), ((64, 96, 128), 5, 6)])
+def test_variant4_projection_epilogue_equals_separate_pass(dims, P, R):
+    opts = sphere_options(dims, P=P, R=R)
+    epi, sep = FireXSim(dims, opts), FireXSim(dims, opts)
+    for s in (epi, sep):
+        s.set_jacobi("resident", V4)
+    sep.set_tiles(0, A.PROJECT_SEPARATE)
+    epi.step(2, DT)
+    sep.step(2, DT)
+    de, ds = epi.diagnostics, sep.diagnostics
+    assert de["jacobi_variant"] == 4 and ds["jacobi_variant"] == 4
+    assert de["project_resident"] == 1 and ds["project_resident"] == 0
+    assert de["launches_per_step"] == ds["launches_per_step"] - 2  # no projection, no divergence launch
+    same(epi, sep)
+
+
+def test_no_projection_epilogue_without_residual_sweeps():
+    dims = (80, 120, 80)
+    g = FireXSim(dims, sphere_options(dims, P=8, R=0))
+    g.set_jacobi("resident", V4)
+    g.step(1, DT)
+    g.sync()
+    assert g.diagnostics["project_resident"] == 0
+    g.close()
+
+
+def test_projection_epilogue_zero_dt_matches_oracle_bit_exact():
+    dims = (96, 144, 96)
+    opts = sphere_options(dims, P=10, R=7)
+    g, o = FireXSim(dims, opts), OracleSim(dims, opts)
+    g.step(3, 0.0)
+    o.step(3, 0.0)
+    assert g.diagnostics["project_resident"] == 1
+    same(g, o)
+
+
+def test_withheld_last_face_expires_the_epilogue_wait():
+    # box 0 withholds its faces from the residual phase's last sweep on: only the epilogue's
+    # halo fetch waits for them
+    dims = (80, 120, 80)
+    opts = sphere_options(dims, P=12, R=12)
+    g = FireXSim(dims, opts)
+    g.set_jacobi("resident", V4)
+    g.step(1, DT)
+    g.sync()
+    assert g.diagnostics["project_resident"] == 1
+    g.set_wait_limit(4096)
+    g.test_hold_face(0, 11)
+    g.step(1, DT)
+    with pytest.raises(FireXError) as e:
+        g.sync()
+    assert e.value.code == A.ERR_TIMEOUT
+    g.close()

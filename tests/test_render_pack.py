@@ -91,7 +91,8 @@ def test_packing_at_step_end_equals_packing_on_read():
     on_read = [g.read(n) for n in ("render_flow", "render_chemistry", "render_media")]
     for a, b in zip(at_step, on_read):
         assert np.array_equal(a, b)
-    assert g.diagnostics["launches_per_step"] == 10  # the packing pass joins the step
+    d = g.diagnostics  # the packing pass joins the step (the residual projection may run in the resident launch)
+    assert d["launches_per_step"] == 10 - d["project_resident"]
 
 
 @pytest.mark.gpu
