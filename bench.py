@@ -362,7 +362,11 @@ def run_gpu(args) -> None:
     # for the resident kernel, K for the fused one
     sweeps_per_launch = (P_ITERS + R_ITERS) * prof_steps / max(1, jac_n)
     peak, peak_kind = measured_peak_hbm()
-    achieved = JACOBI_BYTES_PER_CELL * n_cells * sweeps_per_launch / (jac_avg_ms / 1e3) / 1e9
+    # the resident residual launch may also project the flow (36 B per cell: flow read and
+    # written, the correction read), once per step, spread here over the step's launches
+    epi_bytes = 36 * n_cells * prof_steps / max(1, jac_n) if diag.get("project_resident") else 0
+    alg_bytes = JACOBI_BYTES_PER_CELL * n_cells * sweeps_per_launch + epi_bytes
+    achieved = alg_bytes / (jac_avg_ms / 1e3) / 1e9
     kernel = jacobi_kernel_name(diag)
     traffic = JACOBI_TRAFFIC_PER_LAUNCH.get(kernel)
 
@@ -389,7 +393,8 @@ def run_gpu(args) -> None:
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                          "traffic": traffic, "bytes_per_cell": JACOBI_BYTES_PER_CELL, "avg_launch_us": jac_avg_ms * 1e3,
                          "launches": jac_n, "sweeps_per_launch": sweeps_per_launch,
-                         "algorithmic_bytes_per_launch": JACOBI_BYTES_PER_CELL * n_cells * sweeps_per_launch},
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "projection_epilogue_bytes_per_launch": epi_bytes},
             "passes_ms_per_step": {k: v[0] / prof_steps for k, v in passes.items()},
             "profiled_steps": prof_steps,
             "gpu_launches": int(launches),
