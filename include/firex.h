@@ -378,7 +378,9 @@ int firex_batch_set_staging(firex_batch* batch, int32_t staging);
  * simulate_by = 2, 4 (the default) or 8; 0 restores the default. project: the primary
  * projection and the divergence of its result (the residual's right-hand side,
  * FireXEngine.ts:2256-2257) run as one fused pass (FUSED) or as two (SEPARATE); AUTO fuses
- * them below 8 Mi cells per batch (the recomputed neighbours then come from L2).
+ * them below 8 Mi cells per batch (the recomputed neighbours then come from L2). Unless
+ * SEPARATE, a residual phase run by the resident Jacobi's variant 4 also projects the flow
+ * as its epilogue (no separate projection launch; firex_diagnostics.project_resident).
  * Every choice gives identical results; fire_b200/autotune.py times them. A batch's own
  * setting overrides its members' (0 / AUTO: the first member's). */
 #define FIREX_PROJECT_AUTO 0
