@@ -51,7 +51,11 @@ E2E_MIN_STEPS = 200
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of each Jacobi
 # kernel on this workload, from one ncu capture of that kernel (the same command as this
 # benchmark's default run, one launch captured).
-JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768, "fxk_jacobi_res<float>": 25259264 + 459008}
+# DRAM bytes per launch from captures at HD. The resident kernel: the mean of the step's two
+# launches, the primary phase (25.26 MB + 1.34 MB) and the residual phase with its projection
+# epilogue (63.03 MB + 33.37 MB: the flow read and written once).
+JACOBI_TRAFFIC_PER_LAUNCH: dict = {"fxk_jacobi<float>": 25113088 + 768,
+                                   "fxk_jacobi_res<float>": (25264640 + 1340928 + 63026944 + 33365504) // 2}
 # The two-sweep pass at 508^3 (too large for a capture): one pass (2 sweeps) of a 508x508x128
 # capture moved 266.7 MB + 104.2 MB of DRAM for 33,032,192 cells; the 508^3 figure scales it by
 # the cell count (its traffic grows in proportion: the same tiles and chunks over more planes).
