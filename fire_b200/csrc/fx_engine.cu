@@ -642,7 +642,7 @@ struct firex_batch {
     }
 
     // Fills the brick prefix sums for the launch shape (k, zc); resident boxes when wanted,
-    // of variant resForce when that is 0-3.
+    // of variant resForce when that is 0-4.
     void fill_table(int k, int zc, int zmZc, bool wantRes, int resForce, int simBy) {
         int acc[FX_NSHAPES] = {};
         h->nsims = (int)members.size();

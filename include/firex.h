@@ -397,7 +397,7 @@ typedef struct firex_diagnostics {
     int32_t graph;            /* 1: steps replay a captured CUDA graph */
     int32_t launches_per_step;
     int32_t jacobi_kernel;    /* FIREX_JACOBI_* kernel the last step ran */
-    int32_t jacobi_variant;   /* RESIDENT: the box variant (0-3) it ran; else -1 */
+    int32_t jacobi_variant;   /* RESIDENT: the box variant (0-4) it ran; else -1 */
     int32_t jacobi_staging;   /* two-sweep pass: FIREX_STAGING_TMA or _CPASYNC it ran; else -1 */
     int32_t simulate_by;      /* source-pass bricks of 32 x simulate_by x (8 / simulate_by) cells */
     int32_t project_fused;    /* 1: the primary projection and the residual divergence ran as one pass */

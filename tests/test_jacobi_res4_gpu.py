@@ -180,3 +180,26 @@ def test_withheld_last_face_expires_the_epilogue_wait():
         g.sync()
     assert e.value.code == A.ERR_TIMEOUT
     g.close()
+
+
+def test_projection_epilogue_batch_with_uneven_residual_counts():
+    # each member's boxes run their own residual count, then the epilogue
+    dims_list = [(80, 120, 80), (64, 96, 128), (96, 96, 96)]
+    Rs = [1, 5, 8]
+    alone = []
+    for i, dims in enumerate(dims_list):
+        s = FireXSim(dims, sphere_options(dims, P=9, R=Rs[i], seed=21 + i))
+        s.set_jacobi("unblocked")
+        s.step(2, DT)
+        alone.append(s)
+    members = [FireXSim(d, sphere_options(d, P=9, R=Rs[i], seed=21 + i)) for i, d in enumerate(dims_list)]
+    with FireXBatch() as b:
+        for m in members:
+            b.add(m)
+        b.set_jacobi("resident", V4)
+        b.step(2, DT)
+        b.sync()
+        d = members[0].diagnostics
+        assert d["jacobi_variant"] == 4 and d["project_resident"] == 1
+    for m, s in zip(members, alone):
+        same(m, s)
