@@ -95,7 +95,8 @@ struct Acc {
 
 // One thread per cell of a 32 x BY x (8 / BY) brick (BY = 2, 4 or 8: the tunable brick
 // shape; FX_CELL_BY, 4, by default).
-template <class St, int BY>
+// EARLY: the neighbour terms before the advection (fx_simulate_cell).
+template <class St, int BY, bool EARLY>
 __global__ void __launch_bounds__(256, 3) fxk_simulate(const FxBatchDev* __restrict__ B) {
     constexpr int BX = FX_CELL_BX, BZ = 256 / (FX_CELL_BX * BY);
     // the simulation's parameter block, the uniform entries of its per-step table and its
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(256, 3) fxk_simulate(const FxBatchDev* __restr
         if (x >= S.X || y >= S.Y || z >= S.Z) return;
         const FxGrid g{S.X, S.Y, S.Z};
         Acc<St> a{S.flow[S.fi], S.species[S.si], S.liquid};
-        FxCellOut o = fx_simulate_cell(sP, g, x, y, z, a, S.tab, sUT, sDC);
+        FxCellOut o = fx_simulate_cell<EARLY>(sP, g, x, y, z, a, S.tab, sUT, sDC);
         const int id = x + S.X * (y + S.Y * z);
         fx_st_flow(S.flow[S.fi ^ 1], id, o.flow);
         St::st_species(S.species[S.si ^ 1], id, o.species);
@@ -848,22 +849,27 @@ void fx_launch_step_tables(cudaStream_t s, const FxBatchDev* B, int bricks) {
     fxk_step_tables<<<bricks > 0 ? bricks : 1, 256, 0, s>>>(B);
 }
 
-template <class St, int BY>
+template <class St, int BY, bool EARLY>
 static void launch_simulate(cudaStream_t s, const FxBatchDev* B, int bricks) {
-    static int g = persistent_grid((const void*)fxk_simulate<St, BY>, 256, 1 << 30);
-    fxk_simulate<St, BY><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
+    static int g = persistent_grid((const void*)fxk_simulate<St, BY, EARLY>, 256, 1 << 30);
+    fxk_simulate<St, BY, EARLY><<<bricks < g ? bricks : g, 256, 0, s>>>(B);
 }
 
-template <class St>
+template <class St, bool EARLY>
 static void launch_simulate_shape(cudaStream_t s, int by, const FxBatchDev* B, int bricks) {
-    if (by == 2) launch_simulate<St, 2>(s, B, bricks);
-    else if (by == 8) launch_simulate<St, 8>(s, B, bricks);
-    else launch_simulate<St, 4>(s, B, bricks);
+    if (by == 2) launch_simulate<St, 2, EARLY>(s, B, bricks);
+    else if (by == 8) launch_simulate<St, 8, EARLY>(s, B, bricks);
+    else launch_simulate<St, 4, EARLY>(s, B, bricks);
 }
 
-void fx_launch_simulate(cudaStream_t s, int storage, int by, const FxBatchDev* B, int bricks) {
-    if (storage == FX_STORAGE_MIXED) launch_simulate_shape<StMixed>(s, by, B, bricks);
-    else launch_simulate_shape<StF32>(s, by, B, bricks);
+void fx_launch_simulate(cudaStream_t s, int storage, int by, bool early, const FxBatchDev* B, int bricks) {
+    if (storage == FX_STORAGE_MIXED) {
+        if (early) launch_simulate_shape<StMixed, true>(s, by, B, bricks);
+        else launch_simulate_shape<StMixed, false>(s, by, B, bricks);
+    } else {
+        if (early) launch_simulate_shape<StF32, true>(s, by, B, bricks);
+        else launch_simulate_shape<StF32, false>(s, by, B, bricks);
+    }
 }
 
 void fx_launch_divergence(cudaStream_t s, const FxBatchDev* B, int bricks, int phase) {
