@@ -153,6 +153,9 @@ struct StepPlan {
     bool operator<(const StepPlan& o) const { return key() < o.key(); }
 };
 
+#ifndef FX_SIM_EARLY_CELLS
+#define FX_SIM_EARLY_CELLS (12LL << 20)  // batches below this many cells: the source pass's early order
+#endif
 #ifndef FX_PROJ_RES
 #define FX_PROJ_RES 1  // the residual projection as the resident variant 4's epilogue when it can
 #endif
@@ -758,9 +761,10 @@ struct firex_batch {
         // 0.118 against 0.125 ms)
         const int pf = this->projFuse != FIREX_PROJECT_AUTO ? this->projFuse : members[0]->projFuse;
         p.projDiv = pf == FIREX_PROJECT_FUSED || (pf == FIREX_PROJECT_AUTO && cells < (8LL << 20));
-        // the source pass's neighbour terms ahead of the advection while the fields sit in L2
-        // (measured on B200: HD 0.185 against 0.194 ms per pass; 256^3 1.010 against 0.964)
-        p.simEarly = cells < (8LL << 20);
+        // the source pass's neighbour terms ahead of the advection below 12 Mi cells (measured on
+        // B200, ms per pass, early against reference order: HD 0.185 / 0.194, 160x240x160
+        // 0.353 / 0.361, 192x288x192 0.604 / 0.618; 256^3 1.010 / 0.964)
+        p.simEarly = cells < FX_SIM_EARLY_CELLS;
         if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 2 + resForce : 0) ||
             tableWater != water_signature() || tableSimBy != p.simBy)
             fill_table(p.k, p.zc, p.zmZc, wantRes, resForce, p.simBy);

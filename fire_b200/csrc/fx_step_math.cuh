@@ -303,9 +303,9 @@ FXD FxCellOut fx_simulate_cell(const FxParams& P, const FxGrid& g, int x, int y,
     // temperature gradient of the vorticity confinement, each the reference's expression. EARLY
     // evaluates them before the advection, so that only these values, not the 12 neighbour
     // records, stay live through the update and the neighbour loads overlap the advection's
-    // dependent loads (faster while the fields sit in L2: HD 0.185 against 0.194 ms per pass);
-    // otherwise they are evaluated where the reference does (faster from HBM: 256^3 0.964
-    // against 1.010 ms). The results are the same either way.
+    // dependent loads (faster up to about 10 M cells: HD 0.185 against 0.194 ms per pass,
+    // 192x288x192 0.604 against 0.618); otherwise they are evaluated where the reference does
+    // (256^3: 0.964 against 1.010 ms). The results are the same either way.
     // 6 neighbours with clamped (Neumann) addressing (shaders.ts:43-51)
     const int oL = x > 0 ? id - 1 : id, oR = x < X - 1 ? id + 1 : id;
     const int oB = y > 0 ? id - X : id, oT = y < Y - 1 ? id + X : id;
