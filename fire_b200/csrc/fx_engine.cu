@@ -761,10 +761,11 @@ struct firex_batch {
         // 0.118 against 0.125 ms)
         const int pf = this->projFuse != FIREX_PROJECT_AUTO ? this->projFuse : members[0]->projFuse;
         p.projDiv = pf == FIREX_PROJECT_FUSED || (pf == FIREX_PROJECT_AUTO && cells < (8LL << 20));
-        // the source pass's neighbour terms ahead of the advection below 12 Mi cells (measured on
-        // B200, ms per pass, early against reference order: HD 0.185 / 0.194, 160x240x160
-        // 0.353 / 0.361, 192x288x192 0.604 / 0.618; 256^3 1.010 / 0.964)
-        p.simEarly = cells < FX_SIM_EARLY_CELLS;
+        // the source pass's neighbour terms ahead of the advection below 12 Mi cells with FP32
+        // storage (measured on B200, ms per pass, early against reference order: HD 0.185 /
+        // 0.194, 160x240x160 0.353 / 0.361, 192x288x192 0.604 / 0.618; 256^3 1.010 / 0.964;
+        // mixed storage HD 0.181 / 0.174, 160x240x160 0.344 / 0.326)
+        p.simEarly = p.storage == FX_STORAGE_F32 && cells < FX_SIM_EARLY_CELLS;
         if (tableK != p.k || tableZc != p.zc || tableZmZc != p.zmZc || tableRes != (wantRes ? 2 + resForce : 0) ||
             tableWater != water_signature() || tableSimBy != p.simBy)
             fill_table(p.k, p.zc, p.zmZc, wantRes, resForce, p.simBy);

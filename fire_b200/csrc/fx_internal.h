@@ -15,7 +15,8 @@ void fx_launch_step_begin(cudaStream_t s, FxBatchDev* B);
 void fx_launch_step_end(cudaStream_t s, FxBatchDev* B);
 void fx_launch_step_tables(cudaStream_t s, const FxBatchDev* B, int bricks);
 // The source pass with bricks of 32 x by x (8 / by) cells (by = 2, 4 or 8).
-// early: the neighbour terms before the advection (fx_simulate_cell<EARLY>; same results).
+// early: the neighbour terms before the advection (fx_simulate_cell<EARLY>; same results;
+// FP32 storage only, mixed storage always takes the reference order).
 void fx_launch_simulate(cudaStream_t s, int storage, int by, bool early, const FxBatchDev* B, int bricks);
 void fx_launch_divergence(cudaStream_t s, const FxBatchDev* B, int bricks, int phase);
 void fx_launch_jacobi(cudaStream_t s, bool half, const FxBatchDev* B, int bricks, int phase, int launch, int sweep);
